@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark: clustered points/s of the B200 DBSCAN hot path.
+
+One step = one full DBSCAN job (epsilon grid, neighbour count / core flags,
+union-find, canonical ids, border points) over the n=10,000,000 3-D workload
+(seeded synthetic data with the benchmark's distribution), inputs resident in HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one process per GPU: the path does not shard on one
+job here (one GPU is one rank), so every rank runs an independent replica of the
+job and the value is the points all ranks clustered / the max over ranks of the
+timed device time ("scaling": "weak").
+
+--impl reference times the reference's own OpenMP implementation (built from its
+sources into oracle/_ref/) on the host cores, on a bounded sample of the same
+workload; only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "clustered points/sec"
+UNIT = "points/s"
+HBM_PEAK_FALLBACK = 6650.0  # GB/s, used only without MEASURED_PEAKS.json
+SM_COUNT = 148
+FP32_LANES_PER_SM = 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=2, help="benchmark configuration (1, 2, 3 or 5)")
+    ap.add_argument("--n", type=int, default=None, help="override n (smaller runs for profiling)")
+    ap.add_argument("--full-count", action="store_true", help="exact neighbour counts (no early exit)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=50_000, help="points in the bounded CPU sample")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_PEAK_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) >= 9:
+                for i, nm in enumerate(names):
+                    if s[5 + i].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(val: float, world: int) -> float:
+    if world == 1:
+        return val
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([val], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own OpenMP implementation on the host cores
+# ---------------------------------------------------------------------------
+def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1, warmup: int = 0):
+    import oracle
+
+    if not oracle.have_ref():
+        try:
+            oracle.build("/root/reference" if os.path.isdir("/root/reference") else None)
+        except Exception:
+            pass
+    w = pkg.synthetic.make(config, n=sample_n)
+    if oracle.have_ref():
+        kind = "reference"
+        times = []
+        for i in range(warmup + steps):
+            _, _, _, info = oracle.run_ref(w.coords, w.eps, w.min_pts, threads=threads)
+            if i >= warmup:
+                times.append(info["total_ms"] / 1000.0)
+        cores = threads
+    else:
+        kind = "port"
+        times = []
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            oracle.grid(w.coords, w.eps, w.min_pts)
+            if i >= warmup:
+                times.append(time.perf_counter() - t0)
+        cores = oracle.threads()
+    per_step = sum(times) / len(times)
+    return {
+        "value": w.n / per_step, "unit": UNIT, "cores": cores, "kind": kind,
+        "sample": (f"{w.name} generator at n={w.n} (same eps={w.eps}, minPts={w.min_pts}); "
+                   f"{'reference OpenMP data_process (oracle/_ref)' if kind == 'reference' else 'oracle grid port'}"
+                   f", {cores} threads, {per_step:.2f} s per job; the reference is O(n^2), so its rate at the "
+                   f"full n is lower by about n_full/n_sample"),
+        "seconds_per_step": per_step,
+        "workload": w.name,
+    }
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import importlib
+    pkg = importlib.import_module("nextdbscan-exa_b200")
+    threads = os.cpu_count() or 1
+    cb = cpu_reference(pkg, args.config, args.cpu_sample, threads, steps=args.steps, warmup=args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["seconds_per_step"] * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator, benchmark distribution)",
+        "config": {"workload": cb["workload"], "sample_n": args.cpu_sample, "parallelism": "host OpenMP"},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import importlib
+
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    pkg = importlib.import_module("nextdbscan-exa_b200")
+    w = pkg.synthetic.make(args.config, n=args.n)
+    n, d = w.n, w.d
+    stream = torch.cuda.current_stream()
+    ctx = pkg.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+
+    x = torch.from_numpy(w.coords).cuda()
+    nn = torch.empty(n, dtype=torch.int32, device="cuda")
+    ci = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    full = args.full_count
+    torch.cuda.synchronize()
+
+    def step():
+        return ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(), full_count=full)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+
+    step_ms, stats = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)  # evict L2 between timed steps (not timed)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = step()
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            stats.append(ctx.stats())
+    torch.cuda.synchronize()
+    barrier(world)
+    total_ms = max_over_ranks(sum(step_ms), world)
+    value = world * n * args.steps / (total_ms / 1000.0)
+
+    # end to end through the public API: pinned host input -> device -> pinned host labels
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.from_numpy(w.coords).pin_memory()
+        hnn = torch.empty(n, dtype=torch.int32).pin_memory()
+        hci = torch.empty(n, dtype=torch.int32).pin_memory()
+        for _ in range(2):
+            ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
+                         full_count=full)
+        torch.cuda.synchronize()
+        barrier(world)
+        e_ms = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
+                         full_count=full)
+            e1.record(stream)
+            e1.synchronize()
+            e_ms.append(e0.elapsed_time(e1))
+        e_total = max_over_ranks(sum(e_ms), world)
+        e2e = {"value": world * n * args.steps / (e_total / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": n * d * 4, "d2h_bytes_per_step": 2 * n * 4}
+
+    # roofline of the dominant kernel (device time measured with CUDA events inside the library)
+    hbm_peak, peak_src = peaks()
+    clk_sum = clk.summary()
+    kern = {
+        "count_kernel": statistics.mean(s["ms_count_kernel"] for s in stats),
+        "union_kernel": statistics.mean(s["ms_union_kernel"] for s in stats),
+        "border_kernel": statistics.mean(s["ms_border_kernel"] for s in stats),
+        "radix_sort": statistics.mean(s["ms_sort_kernels"] for s in stats),
+    }
+    s0 = stats[-1]
+    dominant = max(kern, key=kern.get)
+    roof = roofline(dominant, kern[dominant], s0, n, d, hbm_peak, peak_src, clk_sum)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference(pkg, args.config, args.cpu_sample, os.cpu_count() or 1)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    launches = count_launches(s0)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator with the benchmark's distribution)",
+            "config": {"workload": w.name, "n": n, "d": d, "eps": w.eps, "min_pts": w.min_pts,
+                       "counts": "exact" if full else "early-exit at minPts (exact core flags and labels)",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"{world} independent replica(s), one per GPU"},
+            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk_sum,
+            "gpu_launches": launches * args.steps,
+            "result": {"clusters": res.clusters, "noise": res.noise, "core_count": res.core_count},
+            "phases_ms": {k: round(statistics.mean(s[k] for s in stats), 4)
+                          for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
+            "kernels_ms": {k: round(v, 4) for k, v in kern.items()},
+            "pairs": {"count": s0["count_pairs"], "union": s0["union_pairs"], "border": s0["border_pairs"]},
+            "grid": {"cells": s0["n_cells"], "tiles": s0["n_tiles"], "rows": s0["stencil_rows"],
+                     "same_cell_linked": s0["same_cell_linked"], "key_bits": s0["key_bits"]},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def count_launches(s) -> int:
+    """Kernels of one job, as counted by the library at every launch site."""
+    return int(s["kernel_launches"])
+
+
+def roofline(kind, ms, s, n, d, hbm_peak, peak_src, clk):
+    """Algorithmic work of one launch / its device time."""
+    if kind == "radix_sort":
+        kb = s["key_bytes"]
+        # per pass: upsweep reads keys; downsweep reads and writes (key, id)
+        per_pass = n * (kb + 2 * (kb + 4))
+        achieved = per_pass * s["sort_passes"] / (ms / 1000.0) / 1e9
+        return {"kernel": "radix_sort (all passes)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "peak_source": f"{peak_src} hbm_gbs"}
+    pairs = {"count_kernel": s["count_pairs"], "union_kernel": s["union_pairs"],
+             "border_kernel": s["border_pairs"]}[kind]
+    flops = pairs * 3 * d  # separately rounded sub, mul, add per dimension (no FMA credit)
+    achieved = flops / (ms / 1000.0) / 1e12
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak = SM_COUNT * FP32_LANES_PER_SM * mhz * 1e6 / 1e12
+    return {"kernel": kind, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": None,
+            "peak_source": "nominal FP32 issue rate (148 SMs x 128 lanes) at the median sampled SM clock; "
+                           "no FP32 figure in MEASURED_PEAKS.json",
+            "work": f"{pairs} pair predicates x 3d FP32 ops"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,163 @@
+/*
+ * ndb_b200.h -- C ABI of the B200 DBSCAN hot path (libndb_b200.so).
+ *
+ * Drop-in for nextdbscan-exa's algorithm layer, the class data_process
+ * (data_process.h:45-102, data_process.cpp:50-458), which the reference selects at
+ * compile time (data_process.cpp:24-30) and calls from nextdbscan::start
+ * (nextdbscan.cpp:46-58).  Each entry point below names the reference interface it
+ * replaces.  Plain pointers and sizes only; no C++ or CUDA types cross this boundary.
+ *
+ * Conventions
+ *   - Every call returns an ndb_status; the library never exits the process (the
+ *     reference is noexcept everywhere and calls exit() on hard errors).
+ *   - Output buffers are owned by the caller.  Host pointers unless
+ *     NDB_FLAG_DEVICE_PTRS is set, in which case coords and every output array
+ *     are device pointers on the context's device.
+ *   - A context is used by one host thread at a time.  Work is queued on the
+ *     context's stream; calls return after their results are in the caller's
+ *     buffers.
+ *   - Coordinates are FP32, row-major (point-major), n x d, exactly the
+ *     reference's v_coord layout (data_process.h:55, magma_input.h:113-125).
+ *
+ * Result semantics (bit-identical to the reference OpenMP implementation):
+ *   nn[i]             points j (i included) with dist2(i,j) <= eps*eps, where
+ *                     dist2 = 0; dist2 += (a-b)*(a-b) per dimension, every FP32
+ *                     operation separately rounded (data_process.cpp:443-447).
+ *                     Without NDB_FLAG_FULL_COUNT the count of a core point stops
+ *                     early once it reaches min_pts: nn[i] is exact whenever it is
+ *                     below min_pts and is some value >= min_pts otherwise, so the
+ *                     core flags are exact either way.
+ *   cluster_index[i]  NDB_NO_CLUSTER (INT32_MAX, data_process.h:26) for noise; else
+ *                     the rank among core points (index order) of the smallest-index
+ *                     core of the core-connected component; a border point takes the
+ *                     minimum such id over the cores within eps
+ *                     (data_process.cpp:93-266 after convergence).
+ */
+#ifndef NDB_B200_H
+#define NDB_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NDB_NO_CLUSTER INT32_MAX
+
+/* Largest supported dimensionality. */
+#define NDB_MAX_DIM 16
+
+typedef enum ndb_status {
+    NDB_OK = 0,
+    NDB_ERR_INVALID_ARGUMENT = 1, /* null pointer, n < 0, bad flags, ... */
+    NDB_ERR_UNSUPPORTED_DIM = 2,  /* d outside 1..NDB_MAX_DIM */
+    NDB_ERR_INVALID_EPS = 3,      /* eps*eps (FP32) is NaN or infinite */
+    NDB_ERR_TOO_MANY_POINTS = 4,  /* n > NDB_MAX_POINTS */
+    NDB_ERR_OUT_OF_MEMORY = 5,    /* device allocation failed */
+    NDB_ERR_CUDA = 6,             /* a CUDA runtime call failed; see ndb_b200_last_cuda_error */
+    NDB_ERR_NO_DEVICE = 7,        /* no CUDA device / bad device ordinal */
+    NDB_ERR_DEVICE_LIMIT = 8,     /* a device-side loop hit its iteration bound */
+    NDB_ERR_NO_STATE = 9,         /* ndb_b200_assign_labels before ndb_b200_classify */
+    NDB_ERR_BAD_JOB = 10          /* a batched job descriptor is invalid */
+} ndb_status;
+
+/* Largest n per job: indices are int32, as in the reference (data_process.h:47-59). */
+#define NDB_MAX_POINTS 2147483000LL
+
+/* flags */
+#define NDB_FLAG_APPROXIMATE 0x1u  /* reference -a 1 (main.cpp:45, data_process.cpp:215-217).
+                                      Accepted for drop-in compatibility; the union-find
+                                      result is already exact, which is a valid (tight)
+                                      upper bound on the cluster count. */
+#define NDB_FLAG_FULL_COUNT  0x2u  /* exact nn for every point (no early exit at min_pts) */
+#define NDB_FLAG_DEVICE_PTRS 0x4u  /* coords and outputs are device pointers */
+
+/* Mirrors nextdbscan::result (nextdbscan.h:43-48). */
+typedef struct ndb_result {
+    int32_t clusters;
+    int32_t noise;
+    int32_t core_count;
+    int32_t n;
+} ndb_result;
+
+/* Counters of the last run, for measurement (no reference counterpart; the
+ * reference prints phase times from magma_util::measure_duration, magma_util.h:51-64). */
+typedef struct ndb_stats {
+    int64_t n_valid;          /* points that took part in the grid */
+    int64_t n_cells;          /* non-empty grid cells */
+    int64_t n_tiles;          /* work items (cell chunks of up to 32 points) */
+    int32_t grid_dims;        /* gridded dimensions (1..3) */
+    int32_t stencil_rows;     /* neighbour rows per cell */
+    int32_t same_cell_linked; /* 1 when all points of a cell are provably within eps */
+    int32_t key_bits;         /* radix-sort key width actually sorted */
+    int64_t count_pairs;      /* pair predicates evaluated by the neighbour count */
+    int64_t union_pairs;      /* pair predicates evaluated by the union-find */
+    int64_t border_pairs;     /* pair predicates evaluated by the border assignment */
+    float ms_grid;            /* device time of bbox + keys + sort + cells + gather + rows */
+    float ms_count;           /* device time of the neighbour count / core flags */
+    float ms_union;           /* device time of the union-find + canonical ids */
+    float ms_border;          /* device time of the border assignment + meta */
+    float ms_sort_kernels;    /* device time of the radix sort (all passes) */
+    float ms_count_kernel;    /* device time of the neighbour-count kernel */
+    float ms_union_kernel;    /* device time of the union-find kernel */
+    float ms_border_kernel;   /* device time of the border kernel */
+    int32_t sort_passes;      /* radix passes (8 bits each) */
+    int32_t key_bytes;        /* 4 or 8 */
+    int32_t kernel_launches;  /* kernels launched by the last classify + assign_labels */
+} ndb_stats;
+
+typedef struct ndb_ctx ndb_ctx;
+
+/* Creates a context on CUDA device `device` with its own non-blocking stream.
+ * Replaces the construction of data_process (data_process.h:60-77). */
+ndb_status ndb_b200_create(ndb_ctx **ctx, int32_t device);
+
+/* Frees every device buffer of the context. */
+ndb_status ndb_b200_destroy(ndb_ctx *ctx);
+
+/* Use an existing cudaStream_t (passed as void*) instead of the context's own
+ * stream; NULL restores the context's stream. */
+ndb_status ndb_b200_set_stream(ndb_ctx *ctx, void *cuda_stream);
+
+/* Phase 1: epsilon grid, neighbour counting and core flags.
+ * Replaces data_process::select_and_process (data_process.cpp:334-392) and
+ * process_points (data_process.cpp:395-458).  nn_out (n int32) may be NULL.
+ * The grid and the counts stay in the context for ndb_b200_assign_labels. */
+ndb_status ndb_b200_classify(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d,
+                             float eps, int32_t min_pts, uint32_t flags, int32_t *nn_out);
+
+/* Phase 2: union-find over core points, canonical cluster ids, border points and
+ * the result meta.  Replaces data_process::select_cores_and_process
+ * (data_process.cpp:268-332), process_cores (:93-266) and get_result_meta (:50-91).
+ * cluster_index_out (n int32) may be NULL; result may be NULL. */
+ndb_status ndb_b200_assign_labels(ndb_ctx *ctx, int32_t *cluster_index_out, ndb_result *result);
+
+/* Both phases in one call: the body of nextdbscan::start without the file read
+ * (nextdbscan.cpp:46-58). */
+ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps,
+                        int32_t min_pts, uint32_t flags, int32_t *nn_out,
+                        int32_t *cluster_index_out, ndb_result *result);
+
+/* Per-core label array of the last run, the reference's v_cluster_label
+ * (data_process.h:58, filled at data_process.cpp:141-260): entry k is the cluster id
+ * of the k-th core point, so label[k] == k exactly for the reference's roots
+ * (data_process.cpp:79-88).  Host buffer of at least core_count entries. */
+ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capacity);
+
+/* Counters and phase times of the last run. */
+ndb_status ndb_b200_get_stats(ndb_ctx *ctx, ndb_stats *stats);
+
+/* Human-readable text of a status. */
+const char *ndb_b200_strerror(ndb_status status);
+
+/* Text of the last CUDA error seen by this context (empty when none). */
+const char *ndb_b200_last_cuda_error(ndb_ctx *ctx);
+
+/* Library version string. */
+const char *ndb_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NDB_B200_H */

@@ -1,0 +1,782 @@
+// ndb_api.cu -- context, grid planning and the extern "C" entry points of
+// libndb_b200.so (declared in include/ndb_b200.h).
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/ndb_b200.h"
+#include "ndb_internal.h"
+#include "ndb_kernels.cuh"
+
+using namespace ndb;
+
+#define NDB_VERSION "0.1.0"
+
+struct ndb_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string last_cuda_error;
+
+    // inputs / per-point arrays
+    DevBuf coords, keys0, keys1, ids0, ids1, flags, pos, pcell, xs;
+    DevBuf nn_sorted, nn_orig, core_sorted, core_orig, rank, ci_sorted, ci_orig, labels;
+    // per-cell arrays
+    DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid;
+    // union-find
+    DevBuf parent, comp_min;
+    // scratch
+    DevBuf sort_hist, scan_scratch, small;  // small: counters, bbox, scalars
+
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // kernel-level events: sort, count, union, border (begin, end)
+    cudaEvent_t kev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+
+    // state kept between classify and assign_labels
+    bool have_state = false;
+    int64_t n = 0, nv = 0, n_cells = 0, n_items = 0;
+    int d = 0;
+    float e2 = 0.0f;
+    int min_pts = 0;
+    uint32_t flags_run = 0;
+    bool key64 = false;
+    int cell_units = 0;
+    int n_rows = 0;
+    const float *coords_dev = nullptr;  // device coordinates of the current job
+    GridDev grid{};
+    Stencil stencil{};
+    int64_t n_cores = 0;
+    ndb_result result{};
+    bool have_labels = false;
+    ndb_stats stats{};
+};
+
+namespace {
+
+// layout of ctx->small
+constexpr size_t kSmallBboxOff = 0;          // int[2*kMaxDim]
+constexpr size_t kSmallInvalidOff = 256;     // u64
+constexpr size_t kSmallCountersOff = 512;    // u64[8]: 0 clusters 1 noise 2 count pairs 3 union pairs 4 border pairs
+constexpr size_t kSmallScalarOff = 1024;     // u32[8]: 0 n_cells 1 n_items 2 n_cores
+constexpr size_t kSmallErrOff = 1536;        // int
+constexpr size_t kSmallBytes = 2048;
+
+inline unsigned blocks_for(int64_t n, int threads = kBlock) {
+    int64_t b = (n + threads - 1) / threads;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+struct Fail {
+    ndb_status st;
+};
+
+inline void ck(ndb_ctx *ctx, cudaError_t e) {
+    if (e == cudaSuccess) return;
+    ctx->last_cuda_error = cudaGetErrorString(e);
+    throw Fail{e == cudaErrorMemoryAllocation ? NDB_ERR_OUT_OF_MEMORY : NDB_ERR_CUDA};
+}
+
+inline void ensure(ndb_ctx *ctx, DevBuf &b, size_t bytes) { ck(ctx, b.ensure(bytes < 16 ? 16 : bytes)); }
+
+template <typename T>
+T *small_at(ndb_ctx *ctx, size_t off) {
+    return reinterpret_cast<T *>(static_cast<char *>(ctx->small.ptr) + off);
+}
+
+// ---------------------------------------------------------------------------
+// Grid planning (host).
+//
+// r bounds |a_k - b_k| for every dimension k of every pair the FP32 predicate
+// accepts: the rounded square of the rounded difference is <= e2, so the real
+// difference is at most max(sqrt(e2), 2^-63) * (1 + 2^-20).
+//
+// Same-cell-linked grid (d <= 3, e2 >= 2^-100): cubic cells of width
+// w = sqrt(e2 / d * (1 - 2^-10)).  Two points of one cell differ by less than
+// w * (1 + 2^-20) per dimension, so their FP32 length is below
+// d * w^2 * (1 + 2^-19) * (1 + 2^-24)^5 < e2: every pair inside a cell is in range.
+// Otherwise (or when a dimension would need more than the per-dimension cell cap)
+// up to three dimensions are gridded with cells of at least r * (1 + 2^-12).
+//
+// Stencil: cell coordinates of an accepted pair differ by at most
+// R = ceil(r / w + 2^-18) per dimension (the 2^-18 covers the cell-coordinate
+// rounding, < 2^-21 cells); a row of offsets is dropped only when even the
+// closest points of the two cells, min |delta| >= (|o| - 1 - 2^-18) * w per
+// dimension, are further apart than r.
+// ---------------------------------------------------------------------------
+struct Plan {
+    GridDev g{};
+    Stencil st{};
+    bool cell_units = false;
+    int key_bits = 0;
+};
+
+Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
+    Plan pl;
+    double r = sqrt((double)e2);
+    if (r < ldexp(1.0, -63)) r = ldexp(1.0, -63);
+    r *= 1.0 + ldexp(1.0, -20);
+    const double slack = ldexp(1.0, -18);
+
+    auto cap_for = [](int k) { return k >= 3 ? ldexp(1.0, 20) : ldexp(1.0, 30); };
+
+    int k = 0;
+    int dims[3] = {0, 0, 0};
+    double w[3] = {1, 1, 1};
+    bool linked = false;
+    if (d <= 3 && (double)e2 >= ldexp(1.0, -100)) {
+        const double wl = sqrt((double)e2 / d * (1.0 - ldexp(1.0, -10)));
+        bool fits = wl > 0;
+        for (int a = 0; a < d && fits; ++a) fits = (hi[a] - lo[a]) / wl + 1.0 < cap_for(d);
+        if (fits) {
+            k = d;
+            for (int a = 0; a < d; ++a) {
+                dims[a] = a;
+                w[a] = wl;
+            }
+            linked = true;
+        }
+    }
+    if (!linked) {
+        k = d < 3 ? d : 3;
+        std::vector<int> order(d);
+        for (int a = 0; a < d; ++a) order[a] = a;
+        // grid the k widest dimensions, keeping input order among them
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return (hi[x] - lo[x]) > (hi[y] - lo[y]); });
+        std::sort(order.begin(), order.begin() + k);
+        for (int a = 0; a < k; ++a) {
+            dims[a] = order[a];
+            const double span = hi[dims[a]] - lo[dims[a]];
+            w[a] = r * (1.0 + ldexp(1.0, -12));
+            if (span / w[a] + 1.0 >= cap_for(k)) w[a] = span / (cap_for(k) - 2.0);
+        }
+    }
+    pl.cell_units = linked;
+    pl.g.k = k;
+    unsigned long long stride = 1;
+    double total = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (a < k) {
+            const double span = hi[dims[a]] - lo[dims[a]];
+            pl.g.dim[a] = dims[a];
+            pl.g.lo[a] = lo[dims[a]];
+            pl.g.inv_w[a] = 1.0 / w[a];
+            pl.g.g[a] = (long long)floor(span / w[a]) + 1;
+            pl.g.stride[a] = stride;
+            stride *= (unsigned long long)pl.g.g[a];
+            total *= (double)pl.g.g[a];
+        } else {
+            pl.g.dim[a] = 0;
+            pl.g.lo[a] = 0;
+            pl.g.inv_w[a] = 0;
+            pl.g.g[a] = 1;
+            pl.g.stride[a] = stride;
+        }
+    }
+    // key bits: every valid key <= total - 1 < 2^bits - 1 (the all-ones key marks invalid points)
+    int bits = 1;
+    while (bits < 64 && ldexp(1.0, bits) - 1.0 < total) ++bits;
+    pl.key_bits = bits;
+
+    int R[3] = {0, 0, 0};
+    for (int a = 0; a < k; ++a) R[a] = (int)ceil(r / w[a] + slack);
+    struct Row {
+        int o1, o2, xr;
+        double dist2;
+    };
+    std::vector<Row> rows;
+    auto gap = [&](int o, int a) {
+        double q = (double)(o < 0 ? -o : o) - 1.0 - slack;
+        return q > 0 ? q * w[a] : 0.0;
+    };
+    const double r2 = r * r;
+    for (int o2 = -R[2]; o2 <= R[2]; ++o2) {
+        for (int o1 = -R[1]; o1 <= R[1]; ++o1) {
+            const double g1 = k >= 2 ? gap(o1, 1) : 0.0, g2 = k >= 3 ? gap(o2, 2) : 0.0;
+            const double base = g1 * g1 + g2 * g2;
+            if (base > r2) continue;
+            int xr = 0;
+            for (int o0 = 1; o0 <= R[0]; ++o0) {
+                const double g0 = gap(o0, 0);
+                if (base + g0 * g0 <= r2) xr = o0;
+            }
+            rows.push_back({o1, o2, xr, base});
+        }
+    }
+    std::stable_sort(rows.begin(), rows.end(), [](const Row &x, const Row &y) {
+        if (x.dist2 != y.dist2) return x.dist2 < y.dist2;
+        return std::abs(x.o1) + std::abs(x.o2) < std::abs(y.o1) + std::abs(y.o2);
+    });
+    pl.st.n_rows = (int)rows.size();
+    for (size_t i = 0; i < rows.size() && i < (size_t)kMaxRows; ++i)
+        pl.st.rows[i] = make_int4(rows[i].o1, rows[i].o2, rows[i].xr, 0);
+    return pl;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) ms = 0.0f;
+    return ms;
+}
+
+// ---------------------------------------------------------------------------
+// phase 1
+// ---------------------------------------------------------------------------
+template <int D, typename K>
+void classify_grid(ndb_ctx *ctx, const Plan &pl) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = ctx->n;
+    const int64_t nv = ctx->nv;
+    constexpr int P = Stride<D>::P;
+
+    ensure(ctx, ctx->keys0, n * sizeof(K));
+    ensure(ctx, ctx->keys1, n * sizeof(K));
+    ensure(ctx, ctx->ids0, n * sizeof(int32_t));
+    ensure(ctx, ctx->ids1, n * sizeof(int32_t));
+    ensure(ctx, ctx->sort_hist, sort_hist_words(n) * sizeof(uint32_t));
+    const size_t scan_words = std::max(scan_scratch_words(n + 1), scan_scratch_words((int64_t)sort_hist_words(n)));
+    ensure(ctx, ctx->scan_scratch, (scan_words + 64) * sizeof(uint32_t));
+
+    K invalid_key = (K)(pl.key_bits >= (int)(8 * sizeof(K)) ? ~(K)0 : (((K)1 << pl.key_bits) - 1));
+    ++launch_counter(), key_kernel<D, K><<<blocks_for(n), kBlock, 0, st>>>(ctx->coords_dev, n, pl.g, invalid_key,
+                                                        ctx->keys0.as<K>(), ctx->ids0.as<int32_t>());
+    ck(ctx, cudaGetLastError());
+    bool in_first = true;
+    cudaEventRecord(ctx->kev[0], st);
+    if (sizeof(K) == 4)
+        ck(ctx, radix_sort_pairs_u32(reinterpret_cast<uint32_t *>(ctx->keys0.ptr), ctx->ids0.as<int32_t>(),
+                                     reinterpret_cast<uint32_t *>(ctx->keys1.ptr), ctx->ids1.as<int32_t>(), n,
+                                     pl.key_bits, ctx->sort_hist.as<uint32_t>(), ctx->scan_scratch.as<uint32_t>(),
+                                     &in_first, st));
+    else
+        ck(ctx, radix_sort_pairs_u64(reinterpret_cast<uint64_t *>(ctx->keys0.ptr), ctx->ids0.as<int32_t>(),
+                                     reinterpret_cast<uint64_t *>(ctx->keys1.ptr), ctx->ids1.as<int32_t>(), n,
+                                     pl.key_bits, ctx->sort_hist.as<uint32_t>(), ctx->scan_scratch.as<uint32_t>(),
+                                     &in_first, st));
+    cudaEventRecord(ctx->kev[1], st);
+    ctx->stats.sort_passes = (pl.key_bits + 7) / 8;
+    ctx->stats.key_bytes = (int32_t)sizeof(K);
+    if (!in_first) {
+        std::swap(ctx->keys0, ctx->keys1);
+        std::swap(ctx->ids0, ctx->ids1);
+    }
+    const K *keys = ctx->keys0.as<K>();
+    const int32_t *perm = ctx->ids0.as<int32_t>();
+
+    // cells
+    ensure(ctx, ctx->flags, (n + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->pos, (n + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->pcell, (n + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->cell_start, (n + 2) * sizeof(int32_t));
+    ensure(ctx, ctx->cell_key, (n + 1) * sizeof(K));
+    uint32_t *scal = small_at<uint32_t>(ctx, kSmallScalarOff);
+    ++launch_counter(), cell_flag_kernel<K><<<blocks_for(nv), kBlock, 0, st>>>(keys, nv, ctx->flags.as<uint32_t>());
+    ck(ctx, cudaGetLastError());
+    ck(ctx, scan_exclusive_u32(ctx->flags.as<uint32_t>(), ctx->pos.as<uint32_t>(), nv, scal + 0,
+                               ctx->scan_scratch.as<uint32_t>(), st));
+    ++launch_counter(), cell_write_kernel<K><<<blocks_for(nv), kBlock, 0, st>>>(keys, nv, ctx->pos.as<uint32_t>(), scal + 0,
+                                                            ctx->cell_start.as<int32_t>(), ctx->cell_key.as<K>(),
+                                                            ctx->pcell.as<int32_t>());
+    ck(ctx, cudaGetLastError());
+    ensure(ctx, ctx->xs, (nv + 1) * P * sizeof(float));
+    ++launch_counter(), gather_kernel<D><<<blocks_for(nv), kBlock, 0, st>>>(ctx->coords_dev, perm, nv, ctx->xs.as<float>());
+    ck(ctx, cudaGetLastError());
+    uint32_t n_cells32 = 0;
+    ck(ctx, cudaMemcpyAsync(&n_cells32, scal + 0, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+    const int64_t n_cells = n_cells32;
+    ctx->n_cells = n_cells;
+
+    // neighbour rows
+    const int n_rows = pl.st.n_rows;
+    ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
+    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells * n_rows), kBlock, 0, st>>>(ctx->cell_key.as<K>(), n_cells, pl.g, pl.st,
+                                                                  ctx->nbr.as<int2>());
+    ck(ctx, cudaGetLastError());
+
+    // work items
+    ensure(ctx, ctx->item_cnt, (n_cells + 1) * sizeof(uint32_t));
+    ++launch_counter(), item_count_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(ctx->cell_start.as<int32_t>(), n_cells,
+                                                              ctx->item_cnt.as<uint32_t>());
+    ck(ctx, cudaGetLastError());
+    ck(ctx, scan_exclusive_u32(ctx->item_cnt.as<uint32_t>(), ctx->item_cnt.as<uint32_t>(), n_cells, scal + 1,
+                               ctx->scan_scratch.as<uint32_t>(), st));
+    uint32_t n_items32 = 0;
+    ck(ctx, cudaMemcpyAsync(&n_items32, scal + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+    ctx->n_items = n_items32;
+    ensure(ctx, ctx->items, (ctx->n_items + 1) * sizeof(int2));
+    ++launch_counter(), item_write_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(ctx->cell_start.as<int32_t>(), n_cells,
+                                                              ctx->item_cnt.as<uint32_t>(), ctx->items.as<int2>());
+    ck(ctx, cudaGetLastError());
+}
+
+template <int D>
+void count_phase(ndb_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
+    ensure(ctx, ctx->nn_sorted, (ctx->n + 1) * sizeof(int32_t));
+    const bool early = (ctx->flags_run & NDB_FLAG_FULL_COUNT) == 0;
+    const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    cudaEventRecord(ctx->kev[2], st);
+    if (ctx->n_items > 0) {
+        if (early)
+            ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
+                ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
+                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), counters + 2);
+        else
+            ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
+                ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
+                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), counters + 2);
+        ck(ctx, cudaGetLastError());
+    }
+    cudaEventRecord(ctx->kev[3], st);
+}
+
+void core_flags_phase(ndb_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = ctx->n;
+    ensure(ctx, ctx->core_sorted, n + 1);
+    ensure(ctx, ctx->cell_has_core, ctx->n_cells + 1);
+    ensure(ctx, ctx->nn_orig, (n + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->core_orig, (n + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->rank, (n + 1) * sizeof(uint32_t));
+    ck(ctx, cudaMemsetAsync(ctx->cell_has_core.ptr, 0, ctx->n_cells + 1, st));
+    ++launch_counter(), core_flags_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+        ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->min_pts, ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(),
+        ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->nn_orig.as<int32_t>(),
+        ctx->core_orig.as<uint32_t>());
+    ck(ctx, cudaGetLastError());
+}
+
+template <int D>
+void classify_dispatch(ndb_ctx *ctx, const Plan &pl) {
+    if (pl.key_bits <= 32) {
+        ctx->key64 = false;
+        classify_grid<D, uint32_t>(ctx, pl);
+    } else {
+        ctx->key64 = true;
+        classify_grid<D, uint64_t>(ctx, pl);
+    }
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    count_phase<D>(ctx);
+    core_flags_phase(ctx);
+    cudaEventRecord(ctx->ev[2], ctx->stream);
+}
+
+// ---------------------------------------------------------------------------
+// phase 2
+// ---------------------------------------------------------------------------
+template <int D>
+void labels_phase(ndb_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = ctx->n, nv = ctx->nv, n_cells = ctx->n_cells;
+    unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
+    int *err = small_at<int>(ctx, kSmallErrOff);
+    uint32_t *scal = small_at<uint32_t>(ctx, kSmallScalarOff);
+
+    // ranks among cores in input order (data_process.cpp:276-283, :153)
+    ck(ctx, scan_exclusive_u32(ctx->core_orig.as<uint32_t>(), ctx->rank.as<uint32_t>(), n, scal + 2,
+                               ctx->scan_scratch.as<uint32_t>(), st));
+
+    const int64_t n_units = ctx->cell_units ? n_cells : nv;
+    ensure(ctx, ctx->parent, (n_units + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->comp_min, (n_units + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->ci_sorted, (n + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->ci_orig, (n + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->cell_cid, (n_cells + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->labels, (n + 1) * sizeof(int32_t));
+    ++launch_counter(), iota_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units);
+    ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units, kNoCluster);
+    ck(ctx, cudaGetLastError());
+
+    const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    cudaEventRecord(ctx->kev[4], st);
+    if (ctx->n_items > 0) {
+        if (ctx->cell_units)
+            ++launch_counter(), union_cells_kernel<D><<<grid, kBlock, 0, st>>>(
+                ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
+                ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+                ctx->parent.as<int32_t>(), counters + 3, err);
+        else
+            ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
+                ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
+                ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+                ctx->parent.as<int32_t>(), counters + 3, err);
+        ck(ctx, cudaGetLastError());
+    }
+    cudaEventRecord(ctx->kev[5], st);
+    ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(nv, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(),
+                                                       ctx->pcell.as<int32_t>(), ctx->cell_units,
+                                                       ctx->rank.as<uint32_t>(), ctx->parent.as<int32_t>(),
+                                                       ctx->comp_min.as<int32_t>(), err);
+    ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units, err);
+    ++launch_counter(), core_ids_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+        nv, n, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units,
+        ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(), ctx->rank.as<uint32_t>(),
+        ctx->core_orig.as<uint32_t>(), ctx->ci_sorted.as<int32_t>(), ctx->ci_orig.as<int32_t>(), counters);
+    if (ctx->cell_units)
+        ++launch_counter(), cell_ids_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(n_cells, ctx->cell_has_core.as<uint8_t>(),
+                                                                ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(),
+                                                                ctx->cell_cid.as<int32_t>(), counters);
+    ck(ctx, cudaGetLastError());
+    cudaEventRecord(ctx->ev[3], st);
+    cudaEventRecord(ctx->kev[6], st);
+    if (ctx->n_items > 0) {
+        ++launch_counter(), border_kernel<D><<<grid, kBlock, 0, st>>>(
+            ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
+            ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+            ctx->cell_units, ctx->cell_cid.as<int32_t>(), ctx->ids0.as<int32_t>(), ctx->ci_sorted.as<int32_t>(),
+            ctx->ci_orig.as<int32_t>(), counters + 4);
+        ck(ctx, cudaGetLastError());
+    }
+    cudaEventRecord(ctx->kev[7], st);
+    ++launch_counter(), meta_kernel<<<blocks_for(n), kBlock, 0, st>>>(n, ctx->ci_orig.as<int32_t>(), ctx->core_orig.as<uint32_t>(),
+                                                  ctx->rank.as<uint32_t>(), ctx->labels.as<int32_t>(), counters);
+    ck(ctx, cudaGetLastError());
+    cudaEventRecord(ctx->ev[4], st);
+}
+
+ndb_status check_ctx(ndb_ctx *ctx) {
+    if (!ctx) return NDB_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return NDB_ERR_NO_DEVICE;
+    return NDB_OK;
+}
+
+bool is_device_ptr(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <int D>
+ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps, int32_t min_pts, uint32_t flags,
+                         int32_t *nn_out) {
+    cudaStream_t st = ctx->stream;
+    ctx->have_state = false;
+    ctx->have_labels = false;
+    ctx->n = n;
+    ctx->d = D;
+    ctx->e2 = eps * eps;  // data_process.h:73, FP32 product
+    ctx->min_pts = min_pts;
+    ctx->flags_run = flags;
+    ctx->stats = ndb_stats{};
+    launch_counter() = 0;
+    ensure(ctx, ctx->small, kSmallBytes);
+    ck(ctx, cudaMemsetAsync(ctx->small.ptr, 0, kSmallBytes, st));
+    cudaEventRecord(ctx->ev[0], st);
+
+    if (flags & NDB_FLAG_DEVICE_PTRS) {
+        ctx->coords_dev = coords;
+    } else {
+        ensure(ctx, ctx->coords, (size_t)n * D * sizeof(float));
+        ck(ctx, cudaMemcpyAsync(ctx->coords.ptr, coords, (size_t)n * D * sizeof(float), cudaMemcpyHostToDevice, st));
+        ctx->coords_dev = ctx->coords.as<float>();
+    }
+
+    // bounding box of the grid-eligible points
+    int *lo_hi = small_at<int>(ctx, kSmallBboxOff);
+    unsigned long long *n_invalid = small_at<unsigned long long>(ctx, kSmallInvalidOff);
+    ++launch_counter(), bbox_init_kernel<<<1, 32, 0, st>>>(lo_hi, D, n_invalid);
+    ++launch_counter(), bbox_kernel<D><<<std::min<unsigned>(blocks_for(n), 148 * 8), kBlock, 0, st>>>(ctx->coords_dev, n, lo_hi,
+                                                                                  n_invalid);
+    ck(ctx, cudaGetLastError());
+    int h_lo_hi[2 * kMaxDim];
+    unsigned long long h_invalid = 0;
+    ck(ctx, cudaMemcpyAsync(h_lo_hi, lo_hi, 2 * D * sizeof(int), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaMemcpyAsync(&h_invalid, n_invalid, sizeof(h_invalid), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+    ctx->nv = n - (int64_t)h_invalid;
+    double lo[kMaxDim], hi[kMaxDim];
+    for (int a = 0; a < D; ++a) {
+        auto dec = [](int v) {
+            const int i = v >= 0 ? v : v ^ 0x7fffffff;
+            float f;
+            memcpy(&f, &i, sizeof(f));
+            return (double)f;
+        };
+        lo[a] = ctx->nv > 0 ? dec(h_lo_hi[a]) : 0.0;
+        hi[a] = ctx->nv > 0 ? dec(h_lo_hi[D + a]) : 0.0;
+    }
+    const Plan pl = plan_grid(D, ctx->e2, lo, hi);
+    ctx->grid = pl.g;
+    ctx->stencil = pl.st;
+    ctx->n_rows = pl.st.n_rows;
+    ctx->cell_units = pl.cell_units ? 1 : 0;
+    if (pl.st.n_rows > kMaxRows) return NDB_ERR_INVALID_ARGUMENT;
+
+    classify_dispatch<D>(ctx, pl);
+
+    if (nn_out) {
+        if (flags & NDB_FLAG_DEVICE_PTRS)
+            ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+        else
+            ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    }
+    unsigned long long h_counters[8];
+    ck(ctx, cudaMemcpyAsync(h_counters, small_at<unsigned long long>(ctx, kSmallCountersOff), sizeof(h_counters),
+                            cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+    ctx->stats.n_valid = ctx->nv;
+    ctx->stats.n_cells = ctx->n_cells;
+    ctx->stats.n_tiles = ctx->n_items;
+    ctx->stats.grid_dims = pl.g.k;
+    ctx->stats.stencil_rows = pl.st.n_rows;
+    ctx->stats.same_cell_linked = ctx->cell_units;
+    ctx->stats.key_bits = pl.key_bits;
+    ctx->stats.count_pairs = (int64_t)h_counters[2];
+    ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
+    ctx->stats.ms_count = elapsed(ctx->ev[1], ctx->ev[2]);
+    ctx->stats.ms_sort_kernels = elapsed(ctx->kev[0], ctx->kev[1]);
+    ctx->stats.ms_count_kernel = elapsed(ctx->kev[2], ctx->kev[3]);
+    ctx->have_state = true;
+    return NDB_OK;
+}
+
+template <int D>
+ndb_status labels_impl(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
+    cudaStream_t st = ctx->stream;
+    labels_phase<D>(ctx);
+    const int64_t n = ctx->n;
+    if (ci_out) {
+        if (ctx->flags_run & NDB_FLAG_DEVICE_PTRS)
+            ck(ctx, cudaMemcpyAsync(ci_out, ctx->ci_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+        else
+            ck(ctx, cudaMemcpyAsync(ci_out, ctx->ci_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    }
+    unsigned long long h_counters[8];
+    uint32_t h_scal[8];
+    int h_err = 0;
+    ck(ctx, cudaMemcpyAsync(h_counters, small_at<unsigned long long>(ctx, kSmallCountersOff), sizeof(h_counters),
+                            cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaMemcpyAsync(h_scal, small_at<uint32_t>(ctx, kSmallScalarOff), sizeof(h_scal), cudaMemcpyDeviceToHost,
+                            st));
+    ck(ctx, cudaMemcpyAsync(&h_err, small_at<int>(ctx, kSmallErrOff), sizeof(int), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+    if (h_err) return NDB_ERR_DEVICE_LIMIT;
+    ctx->n_cores = h_scal[2];
+    ctx->result.clusters = (int32_t)h_counters[0];
+    ctx->result.noise = (int32_t)h_counters[1];
+    ctx->result.core_count = (int32_t)ctx->n_cores;
+    ctx->result.n = (int32_t)n;
+    ctx->stats.union_pairs = (int64_t)h_counters[3];
+    ctx->stats.border_pairs = (int64_t)h_counters[4];
+    ctx->stats.ms_union = elapsed(ctx->ev[2], ctx->ev[3]);
+    ctx->stats.ms_border = elapsed(ctx->ev[3], ctx->ev[4]);
+    ctx->stats.ms_union_kernel = elapsed(ctx->kev[4], ctx->kev[5]);
+    ctx->stats.ms_border_kernel = elapsed(ctx->kev[6], ctx->kev[7]);
+    ctx->stats.kernel_launches = launch_counter();
+    ctx->have_labels = true;
+    if (result) *result = ctx->result;
+    return NDB_OK;
+}
+
+template <int D>
+ndb_status classify_entry(ndb_ctx *ctx, const float *coords, int64_t n, float eps, int32_t m, uint32_t flags,
+                          int32_t *nn_out) {
+    try {
+        return classify_impl<D>(ctx, coords, n, eps, m, flags, nn_out);
+    } catch (const Fail &f) {
+        ctx->have_state = false;
+        return f.st;
+    }
+}
+
+template <int D>
+ndb_status labels_entry(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
+    try {
+        return labels_impl<D>(ctx, ci_out, result);
+    } catch (const Fail &f) {
+        return f.st;
+    }
+}
+
+#define NDB_DISPATCH_D(d, CALL)  \
+    switch (d) {                 \
+        case 1: return CALL(1);  \
+        case 2: return CALL(2);  \
+        case 3: return CALL(3);  \
+        case 4: return CALL(4);  \
+        case 5: return CALL(5);  \
+        case 6: return CALL(6);  \
+        case 7: return CALL(7);  \
+        case 8: return CALL(8);  \
+        case 9: return CALL(9);  \
+        case 10: return CALL(10); \
+        case 11: return CALL(11); \
+        case 12: return CALL(12); \
+        case 13: return CALL(13); \
+        case 14: return CALL(14); \
+        case 15: return CALL(15); \
+        case 16: return CALL(16); \
+        default: return NDB_ERR_UNSUPPORTED_DIM; \
+    }
+
+}  // namespace
+
+extern "C" {
+
+ndb_status ndb_b200_create(ndb_ctx **out, int32_t device) {
+    if (!out) return NDB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        return NDB_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return NDB_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return NDB_ERR_NO_DEVICE;
+    ndb_ctx *ctx = new ndb_ctx();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return NDB_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    for (auto &e : ctx->ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            delete ctx;
+            return NDB_ERR_CUDA;
+        }
+    }
+    for (auto &e : ctx->kev) {
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            delete ctx;
+            return NDB_ERR_CUDA;
+        }
+    }
+    *out = ctx;
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
+    if (!ctx) return NDB_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    DevBuf *bufs[] = {&ctx->coords,      &ctx->keys0,     &ctx->keys1,      &ctx->ids0,        &ctx->ids1,
+                      &ctx->flags,       &ctx->pos,       &ctx->pcell,      &ctx->xs,          &ctx->nn_sorted,
+                      &ctx->nn_orig,     &ctx->core_sorted, &ctx->core_orig, &ctx->rank,       &ctx->ci_sorted,
+                      &ctx->ci_orig,     &ctx->labels,    &ctx->cell_start, &ctx->cell_key,    &ctx->nbr,
+                      &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
+                      &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small};
+    for (DevBuf *b : bufs) b->release();
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : ctx->kev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_set_stream(ndb_ctx *ctx, void *stream) {
+    if (!ctx) return NDB_ERR_INVALID_ARGUMENT;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_classify(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
+                             uint32_t flags, int32_t *nn_out) {
+    ndb_status s = check_ctx(ctx);
+    if (s != NDB_OK) return s;
+    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS)) return NDB_ERR_INVALID_ARGUMENT;
+    if (n < 0) return NDB_ERR_INVALID_ARGUMENT;
+    if (n > NDB_MAX_POINTS) return NDB_ERR_TOO_MANY_POINTS;
+    if (d < 1 || d > NDB_MAX_DIM) return NDB_ERR_UNSUPPORTED_DIM;
+    if (n > 0 && !coords) return NDB_ERR_INVALID_ARGUMENT;
+    const float e2 = eps * eps;
+    if (!isfinite(e2)) return NDB_ERR_INVALID_EPS;
+    if ((flags & NDB_FLAG_DEVICE_PTRS) && n > 0) {
+        if (!is_device_ptr(coords)) return NDB_ERR_INVALID_ARGUMENT;
+        if (nn_out && !is_device_ptr(nn_out)) return NDB_ERR_INVALID_ARGUMENT;
+    }
+    if (n == 0) {
+        ctx->have_state = true;
+        ctx->have_labels = false;
+        ctx->n = 0;
+        ctx->nv = 0;
+        ctx->n_cells = 0;
+        ctx->n_items = 0;
+        ctx->d = d;
+        ctx->min_pts = min_pts;
+        ctx->flags_run = flags;
+        ctx->stats = ndb_stats{};
+        return NDB_OK;
+    }
+#define NDB_CLASSIFY(D) classify_entry<D>(ctx, coords, n, eps, min_pts, flags, nn_out)
+    NDB_DISPATCH_D(d, NDB_CLASSIFY)
+#undef NDB_CLASSIFY
+}
+
+ndb_status ndb_b200_assign_labels(ndb_ctx *ctx, int32_t *cluster_index_out, ndb_result *result) {
+    ndb_status s = check_ctx(ctx);
+    if (s != NDB_OK) return s;
+    if (!ctx->have_state) return NDB_ERR_NO_STATE;
+    if (ctx->n == 0) {
+        ctx->result = ndb_result{0, 0, 0, 0};
+        ctx->n_cores = 0;
+        ctx->have_labels = true;
+        if (result) *result = ctx->result;
+        return NDB_OK;
+    }
+    if ((ctx->flags_run & NDB_FLAG_DEVICE_PTRS) && cluster_index_out && !is_device_ptr(cluster_index_out))
+        return NDB_ERR_INVALID_ARGUMENT;
+#define NDB_LABELS(D) labels_entry<D>(ctx, cluster_index_out, result)
+    NDB_DISPATCH_D(ctx->d, NDB_LABELS)
+#undef NDB_LABELS
+}
+
+ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
+                        uint32_t flags, int32_t *nn_out, int32_t *cluster_index_out, ndb_result *result) {
+    ndb_status s = ndb_b200_classify(ctx, coords, n, d, eps, min_pts, flags, nn_out);
+    if (s != NDB_OK) return s;
+    return ndb_b200_assign_labels(ctx, cluster_index_out, result);
+}
+
+ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capacity) {
+    ndb_status s = check_ctx(ctx);
+    if (s != NDB_OK) return s;
+    if (!ctx->have_labels) return NDB_ERR_NO_STATE;
+    if (capacity < ctx->n_cores || (ctx->n_cores > 0 && !label_out)) return NDB_ERR_INVALID_ARGUMENT;
+    if (ctx->n_cores == 0) return NDB_OK;
+    if (cudaMemcpyAsync(label_out, ctx->labels.ptr, ctx->n_cores * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                        ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return NDB_ERR_CUDA;
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_get_stats(ndb_ctx *ctx, ndb_stats *stats) {
+    if (!ctx || !stats) return NDB_ERR_INVALID_ARGUMENT;
+    *stats = ctx->stats;
+    return NDB_OK;
+}
+
+const char *ndb_b200_strerror(ndb_status s) {
+    switch (s) {
+        case NDB_OK: return "ok";
+        case NDB_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case NDB_ERR_UNSUPPORTED_DIM: return "unsupported dimensionality (1..16)";
+        case NDB_ERR_INVALID_EPS: return "eps*eps is not a finite float";
+        case NDB_ERR_TOO_MANY_POINTS: return "too many points for int32 indices";
+        case NDB_ERR_OUT_OF_MEMORY: return "device out of memory";
+        case NDB_ERR_CUDA: return "CUDA error";
+        case NDB_ERR_NO_DEVICE: return "no CUDA device";
+        case NDB_ERR_DEVICE_LIMIT: return "device-side iteration bound reached";
+        case NDB_ERR_NO_STATE: return "no classified job in this context";
+        case NDB_ERR_BAD_JOB: return "invalid batched job descriptor";
+    }
+    return "unknown status";
+}
+
+const char *ndb_b200_last_cuda_error(ndb_ctx *ctx) { return ctx ? ctx->last_cuda_error.c_str() : ""; }
+
+const char *ndb_b200_version(void) { return NDB_VERSION; }
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+// ndb_common.cuh -- device helpers shared by the DBSCAN kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ndb {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kNoCluster = 0x7fffffff;
+constexpr int kMaxDim = 16;
+constexpr int kMaxRows = 64;        // stencil rows (3-D same-cell grid: 25, 3-D eps grid: 9)
+constexpr int kTile = 32;           // points of one cell handled by one warp item
+
+// Sorted coordinates are stored point-major with a padded stride so that one
+// point is one (or a few) 8/16-byte vector loads.
+template <int D>
+struct Stride {
+    static constexpr int P = (D <= 2) ? D : ((D + 3) / 4) * 4;
+};
+
+// The reference's predicate (data_process.cpp:443-447): length starts at 0 and
+// accumulates (a-b)*(a-b) dimension by dimension; every operation is separately
+// rounded (no FMA contraction), and the pair is in range iff length <= e2.
+template <int D>
+__device__ __forceinline__ bool in_range(const float (&a)[D], const float (&b)[D], float e2) {
+    float len = 0.0f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const float t = __fsub_rn(a[k], b[k]);
+        len = __fadd_rn(len, __fmul_rn(t, t));
+    }
+    return len <= e2;
+}
+
+template <int D>
+__device__ __forceinline__ void load_point(const float *__restrict__ xs, int64_t idx, float (&x)[D]) {
+    constexpr int P = Stride<D>::P;
+    const float *p = xs + idx * P;
+    if constexpr (P == 1) {
+        x[0] = __ldg(p);
+    } else if constexpr (P == 2) {
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+        x[0] = v.x;
+        x[1] = v.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < P / 4; ++q) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(p) + q);
+            if (4 * q + 0 < D) x[4 * q + 0] = v.x;
+            if (4 * q + 1 < D) x[4 * q + 1] = v.y;
+            if (4 * q + 2 < D) x[4 * q + 2] = v.z;
+            if (4 * q + 3 < D) x[4 * q + 3] = v.w;
+        }
+    }
+}
+
+// Point from shared memory (same padded stride), read as a warp-wide broadcast.
+template <int D>
+__device__ __forceinline__ void load_point_smem(const float *p, float (&x)[D]) {
+    constexpr int P = Stride<D>::P;
+    if constexpr (P == 1) {
+        x[0] = p[0];
+    } else if constexpr (P == 2) {
+        const float2 v = *reinterpret_cast<const float2 *>(p);
+        x[0] = v.x;
+        x[1] = v.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < P / 4; ++q) {
+            const float4 v = reinterpret_cast<const float4 *>(p)[q];
+            if (4 * q + 0 < D) x[4 * q + 0] = v.x;
+            if (4 * q + 1 < D) x[4 * q + 1] = v.y;
+            if (4 * q + 2 < D) x[4 * q + 2] = v.z;
+            if (4 * q + 3 < D) x[4 * q + 3] = v.w;
+        }
+    }
+}
+
+template <int D>
+__device__ __forceinline__ void store_point_smem(float *p, const float (&x)[D]) {
+    constexpr int P = Stride<D>::P;
+#pragma unroll
+    for (int k = 0; k < P; ++k) p[k] = (k < D) ? x[k] : 0.0f;
+}
+
+template <int D>
+__device__ __forceinline__ void fill_nan(float (&x)[D]) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) x[k] = __int_as_float(0x7fc00000);
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// Lock-free union-find over int32 ids.  parent[x] <= x always (the larger root
+// is hooked under the smaller), so every find terminates.  Reads go through L2
+// (ld.cg) because other SMs rewrite parents concurrently.
+// ---------------------------------------------------------------------------
+constexpr int kUfMaxSteps = 1 << 26;
+
+__device__ __forceinline__ int uf_find(int *parent, int x, int *err) {
+    int p = __ldcg(parent + x);
+    int steps = 0;
+    while (p != x) {
+        const int gp = __ldcg(parent + p);
+        if (gp != p) __stcg(parent + x, gp);  // path halving: gp is an ancestor of x
+        x = p;
+        p = gp;
+        if (++steps > kUfMaxSteps) {
+            atomicExch(err, 1);
+            break;
+        }
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_union(int *parent, int a, int b, int *err) {
+    for (int it = 0; it < kUfMaxSteps; ++it) {
+        a = uf_find(parent, a, err);
+        b = uf_find(parent, b, err);
+        if (a == b) return;
+        if (a > b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        const int old = atomicCAS(parent + b, b, a);
+        if (old == b) return;
+    }
+    atomicExch(err, 1);
+}
+
+}  // namespace ndb

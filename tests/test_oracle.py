@@ -1,0 +1,97 @@
+"""The oracle is pinned to the reference before anything is checked against it.
+
+Every fixture under tests/golden/ holds outputs of nextdbscan-exa's own OpenMP
+implementation (made by tests/golden/make_golden.py); both C restatements must
+reproduce them bit for bit.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN, golden_names, load_golden, roots_of
+
+NAMES = golden_names()
+
+
+def test_golden_present():
+    assert len(NAMES) >= 20
+    assert os.path.exists(os.path.join(GOLDEN, "c1_full.json"))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_literal_restatement_matches_reference(name):
+    g = load_golden(name)
+    nn, ci, lab, meta = oracle.reference(g["coords"], float(g["eps"]), int(g["min_pts"]))
+    np.testing.assert_array_equal(nn, g["nn"])
+    np.testing.assert_array_equal(ci, g["cluster_index"])
+    np.testing.assert_array_equal(roots_of(lab), roots_of(g["cluster_label"]))
+    assert [meta["clusters"], meta["noise"], meta["cores"], meta["n"]] == list(g["meta"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_literal_restatement_matches_reference_approximate(name):
+    """-a 1 (data_process.cpp:215-217) is schedule dependent; pinned single threaded."""
+    g = load_golden(name)
+    nn, ci, lab, meta = oracle.reference(g["coords"], float(g["eps"]), int(g["min_pts"]), approximate=True)
+    np.testing.assert_array_equal(ci, g["approx_cluster_index"])
+    np.testing.assert_array_equal(roots_of(lab), roots_of(g["approx_cluster_label"]))
+    assert [meta["clusters"], meta["noise"], meta["cores"], meta["n"]] == list(g["approx_meta"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_grid_restatement_matches_reference(name):
+    g = load_golden(name)
+    e = np.float32(g["eps"])
+    if not np.isfinite(np.float32(e * e)):
+        pytest.skip("grid restatement needs a finite eps*eps")
+    nn, ci, meta = oracle.grid(g["coords"], float(e), int(g["min_pts"]))
+    np.testing.assert_array_equal(nn, g["nn"])
+    np.testing.assert_array_equal(ci, g["cluster_index"])
+    assert [meta["clusters"], meta["noise"], meta["cores"], meta["n"]] == list(g["meta"])
+
+
+def test_grid_restatement_matches_reference_full_c1(pkg):
+    """100,000-point 2-D workload against hashes of the reference's own outputs."""
+    with open(os.path.join(GOLDEN, "c1_full.json")) as f:
+        doc = json.load(f)
+    w = pkg.synthetic.config1()
+    assert hashlib.sha256(w.coords.astype("<f4").tobytes()).hexdigest() == doc["coords_sha256"], \
+        "generator drift: synthetic.config1 no longer reproduces the fixture input"
+    nn, ci, meta = oracle.grid(w.coords, w.eps, w.min_pts)
+    assert hashlib.sha256(nn.astype("<i4").tobytes()).hexdigest() == doc["nn_sha256"]
+    assert hashlib.sha256(ci.astype("<i4").tobytes()).hexdigest() == doc["cluster_index_sha256"]
+    assert (meta["clusters"], meta["noise"], meta["cores"]) == (doc["clusters"], doc["noise"], doc["cores"])
+
+
+def test_grid_matches_literal_random():
+    """Extra agreement between the two restatements on unseeded shapes."""
+    rng = np.random.default_rng(99)
+    for d in (1, 2, 3, 6, 12):
+        x = (rng.uniform(0, 8, (1200, d)) + rng.normal(0, 0.2, (1200, d))).astype(np.float32)
+        for eps, m in ((0.5, 3), (1.0, 6)):
+            a = oracle.reference(x, eps, m)
+            b = oracle.grid(x, eps, m)
+            np.testing.assert_array_equal(a[0], b[0])
+            np.testing.assert_array_equal(a[1], b[1])
+
+
+def test_oracle_planted_mistake_is_caught():
+    """A wrong answer planted in the oracle's output is detected by the comparison."""
+    g = load_golden("c1_n4000")
+    nn, ci, meta = oracle.grid(g["coords"], float(g["eps"]), int(g["min_pts"]))
+    bad = ci.copy()
+    i = int(np.nonzero(bad != oracle.NO_CLUSTER)[0][0])
+    bad[i] += 1
+    assert not np.array_equal(bad, g["cluster_index"])
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference harness not built here")
+def test_reference_harness_reproduces_fixture():
+    g = load_golden("blobs_d3")
+    nn, ci, lab, info = oracle.run_ref(g["coords"], float(g["eps"]), int(g["min_pts"]), threads=2)
+    np.testing.assert_array_equal(nn, g["nn"])
+    np.testing.assert_array_equal(ci, g["cluster_index"])
