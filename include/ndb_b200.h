@@ -156,6 +156,26 @@ const char *ndb_b200_last_cuda_error(ndb_ctx *ctx);
 /* Library version string. */
 const char *ndb_b200_version(void);
 
+/* Largest job ndb_b200_run_noalloc accepts. */
+#define NDB_NOALLOC_MAX_POINTS 32768
+
+/* ndb_b200_run for callers that may not allocate device memory -- a service that
+ * reserves its GPU memory once at start-up and forbids cudaMalloc later, or a host
+ * program that only lends out buffers it owns.  No counterpart in the reference.
+ * Every scratch buffer comes from one fixed device array inside the library (about
+ * 12 MiB, held by every GPU that loads the library until the process exits); the
+ * call makes no cudaMalloc or cudaFree.  coords, nn_out and cluster_index_out are
+ * device pointers on the current device (outputs may be NULL); the work runs on
+ * cuda_stream (NULL: the legacy default stream) and is complete when the call
+ * returns.  n above NDB_NOALLOC_MAX_POINTS returns NDB_ERR_TOO_MANY_POINTS.
+ * The first call on a device does the set-up (it looks up the array's device
+ * address and creates the shared state's timing events), so make it before any
+ * stream capture.  Calls share the array: they are serialised per device, and GPU
+ * work that overlaps a call and touches the same array would race. */
+ndb_status ndb_b200_run_noalloc(const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
+                                uint32_t flags, int32_t *nn_out, int32_t *cluster_index_out,
+                                ndb_result *result, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -780,3 +781,136 @@ const char *ndb_b200_last_cuda_error(ndb_ctx *ctx) { return ctx ? ctx->last_cuda
 const char *ndb_b200_version(void) { return NDB_VERSION; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point (ndb_b200_run_noalloc).
+//
+// Some callers cannot allocate device memory: a service that reserves its GPU
+// memory once at start-up and forbids cudaMalloc afterwards (so a late request can
+// never fail or fragment the pool), code running where an allocation would
+// synchronise the device at the wrong moment, or a plugin host that hands out
+// only the buffers it owns.  For them this entry point runs the same pipeline as
+// ndb_b200_run with every scratch buffer carved out of one file-scope device
+// array of fixed size, so no call allocates.
+//
+// The array lives in the library image: every GPU that loads the library holds
+// it until the process exits.  All calls share it and it keeps the last call's
+// contents; the pipeline clears what must start at zero itself.  Calls are
+// serialised on the host per device and each returns only after its work is
+// done; work the caller enqueues on the GPU around a call must not overlap it,
+// since two overlapping users of the array would race.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t na_align(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kNaN = NDB_NOALLOC_MAX_POINTS;
+constexpr int kNaMaxRows = 25;  // largest stencil plan_grid builds (3-D, same-cell-linked cells)
+
+// Capacity of each buffer for jobs of up to kNaN points (upper bounds of the
+// requests the pipeline makes: keys may be 64-bit, coordinates padded to 16).
+enum NaBuf {
+    NA_KEYS0, NA_KEYS1, NA_IDS0, NA_IDS1, NA_FLAGS, NA_POS, NA_PCELL, NA_XS, NA_NN_SORTED, NA_NN_ORIG,
+    NA_CORE_SORTED, NA_CORE_ORIG, NA_RANK, NA_CI_SORTED, NA_CI_ORIG, NA_LABELS, NA_CELL_START, NA_CELL_KEY,
+    NA_NBR, NA_ITEM_CNT, NA_ITEMS, NA_CELL_HAS_CORE, NA_CELL_CID, NA_PARENT, NA_COMP_MIN, NA_SORT_HIST,
+    NA_SCAN, NA_SMALL, NA_COUNT
+};
+
+constexpr size_t na_cap(int b) {
+    return b == NA_KEYS0 || b == NA_KEYS1 ? 8 * kNaN
+         : b == NA_IDS0 || b == NA_IDS1 ? 4 * kNaN
+         : b == NA_XS ? 4 * 16 * (kNaN + 1)
+         : b == NA_CELL_START ? 4 * (kNaN + 2)
+         : b == NA_CELL_KEY || b == NA_ITEMS ? 8 * (kNaN + 1)
+         : b == NA_NBR ? 8 * (kMaxRows > kNaMaxRows ? kNaMaxRows : kMaxRows) * kNaN + 8
+         : b == NA_CORE_SORTED || b == NA_CELL_HAS_CORE ? kNaN + 1
+         : b == NA_SORT_HIST ? 4 * 256 * ((kNaN + kSortTile - 1) / kSortTile)
+         : b == NA_SCAN ? 4 * 4096
+         : b == NA_SMALL ? 2048
+         : 4 * (kNaN + 1);
+}
+
+constexpr size_t na_offset(int b) { return b == 0 ? 0 : na_offset(b - 1) + na_align(na_cap(b - 1)); }
+constexpr size_t kNaBytes = na_offset(NA_COUNT);
+
+struct NoAllocState {
+    std::mutex mu;
+    bool ready = false;
+    unsigned char *base = nullptr;
+    ndb_ctx ctx;
+};
+
+constexpr int kNaMaxDevices = 64;
+NoAllocState g_na_state[kNaMaxDevices];
+
+DevBuf *na_buf(ndb_ctx &c, int b) {
+    DevBuf *bufs[NA_COUNT] = {&c.keys0,       &c.keys1,     &c.ids0,      &c.ids1,         &c.flags,
+                              &c.pos,         &c.pcell,     &c.xs,        &c.nn_sorted,    &c.nn_orig,
+                              &c.core_sorted, &c.core_orig, &c.rank,      &c.ci_sorted,    &c.ci_orig,
+                              &c.labels,      &c.cell_start, &c.cell_key, &c.nbr,          &c.item_cnt,
+                              &c.items,       &c.cell_has_core, &c.cell_cid, &c.parent,    &c.comp_min,
+                              &c.sort_hist,   &c.scan_scratch, &c.small};
+    return bufs[b];
+}
+
+// Points every buffer of the shared context back at its slice of the array
+// (the pipeline swaps the ping-pong sort buffers between calls).
+void na_carve(NoAllocState &s) {
+    for (int b = 0; b < NA_COUNT; ++b) {
+        DevBuf *d = na_buf(s.ctx, b);
+        d->ptr = s.base + na_offset(b);
+        d->bytes = na_cap(b);
+    }
+}
+
+bool na_inside(const NoAllocState &s, const ndb_ctx &c) {
+    for (int b = 0; b < NA_COUNT; ++b) {
+        const DevBuf *d = na_buf(const_cast<ndb_ctx &>(c), b);
+        const unsigned char *p = static_cast<const unsigned char *>(d->ptr);
+        if (p < s.base || p + d->bytes > s.base + kNaBytes) return false;
+    }
+    return c.coords.ptr == nullptr;
+}
+
+}  // namespace
+
+// The scratch of ndb_b200_run_noalloc: file scope, fixed size, no allocation.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+extern "C" ndb_status ndb_b200_run_noalloc(const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
+                                           uint32_t flags, int32_t *nn_out, int32_t *cluster_index_out,
+                                           ndb_result *result, void *cuda_stream) {
+    if (n < 0 || d < 1) return d < 1 ? NDB_ERR_UNSUPPORTED_DIM : NDB_ERR_INVALID_ARGUMENT;
+    if (n > (int64_t)kNaN) return NDB_ERR_TOO_MANY_POINTS;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) {
+        cudaGetLastError();
+        return NDB_ERR_NO_DEVICE;
+    }
+    NoAllocState &s = g_na_state[dev];
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.ready) {
+        // once per device, with that device current: the host-side name of the array
+        // is not a device address, so look the address up
+        void *addr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+        if (e != cudaSuccess || addr == nullptr) {
+            s.ctx.last_cuda_error = cudaGetErrorString(e);
+            cudaGetLastError();
+            return NDB_ERR_CUDA;
+        }
+        for (auto &ev : s.ctx.ev)
+            if (cudaEventCreate(&ev) != cudaSuccess) return NDB_ERR_CUDA;
+        for (auto &ev : s.ctx.kev)
+            if (cudaEventCreate(&ev) != cudaSuccess) return NDB_ERR_CUDA;
+        s.base = static_cast<unsigned char *>(addr);
+        s.ctx.device = dev;
+        s.ready = true;
+    }
+    na_carve(s);
+    s.ctx.own_stream = nullptr;
+    s.ctx.stream = static_cast<cudaStream_t>(cuda_stream);
+    ndb_status st = ndb_b200_classify(&s.ctx, coords, n, d, eps, min_pts, flags | NDB_FLAG_DEVICE_PTRS, nn_out);
+    if (st == NDB_OK) st = ndb_b200_assign_labels(&s.ctx, cluster_index_out, result);
+    if (!na_inside(s, s.ctx)) st = NDB_ERR_OUT_OF_MEMORY;  // a request outgrew its slice
+    return st;
+}
