@@ -26,7 +26,7 @@ struct ndb_ctx {
     DevBuf coords, keys0, keys1, ids0, ids1, flags, pos, pcell, xs;
     DevBuf nn_sorted, nn_orig, core_sorted, core_orig, rank, ci_sorted, ci_orig, labels;
     // per-cell arrays
-    DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid;
+    DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid, hash_keys, hash_vals, cell_x;
     // union-find
     DevBuf parent, comp_min;
     // scratch
@@ -46,6 +46,7 @@ struct ndb_ctx {
     bool key64 = false;
     int cell_units = 0;
     int n_rows = 0;
+    int n_near_rows = 0;
     const float *coords_dev = nullptr;  // device coordinates of the current job
     GridDev grid{};
     Stencil stencil{};
@@ -63,7 +64,8 @@ constexpr size_t kSmallInvalidOff = 256;     // u64
 constexpr size_t kSmallCountersOff = 512;    // u64[8]: 0 clusters 1 noise 2 count pairs 3 union pairs 4 border pairs
 constexpr size_t kSmallScalarOff = 1024;     // u32[8]: 0 n_cells 1 n_items 2 n_cores
 constexpr size_t kSmallErrOff = 1536;        // int
-constexpr size_t kSmallBytes = 2048;
+constexpr size_t kSmallStencilOff = 2048;    // int4[kMaxRows]: stencil rows of the current job
+constexpr size_t kSmallBytes = 4096;
 
 inline unsigned blocks_for(int64_t n, int threads = kBlock) {
     int64_t b = (n + threads - 1) / threads;
@@ -112,6 +114,7 @@ struct Plan {
     Stencil st{};
     bool cell_units = false;
     int key_bits = 0;
+    int n_near_rows = 0;  // leading rows whose cells are all adjacent in dimensions 1, 2 (|o1|, |o2| <= 1)
 };
 
 Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
@@ -212,8 +215,10 @@ Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
         return std::abs(x.o1) + std::abs(x.o2) < std::abs(y.o1) + std::abs(y.o2);
     });
     pl.st.n_rows = (int)rows.size();
-    for (size_t i = 0; i < rows.size() && i < (size_t)kMaxRows; ++i)
+    for (size_t i = 0; i < rows.size() && i < (size_t)kMaxRows; ++i) {
         pl.st.rows[i] = make_int4(rows[i].o1, rows[i].o2, rows[i].xr, 0);
+        if (std::abs(rows[i].o1) <= 1 && std::abs(rows[i].o2) <= 1 && (int)i == pl.n_near_rows) ++pl.n_near_rows;
+    }
     return pl;
 }
 
@@ -291,11 +296,25 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     const int64_t n_cells = n_cells32;
     ctx->n_cells = n_cells;
 
-    // neighbour rows
+    // neighbour rows, through a hash table of the cells
     const int n_rows = pl.st.n_rows;
+    int64_t hsize = 1024;
+    while (hsize < 2 * n_cells) hsize <<= 1;
+    ensure(ctx, ctx->hash_keys, hsize * sizeof(K));
+    ensure(ctx, ctx->hash_vals, hsize * sizeof(int32_t));
+    ++launch_counter(), hash_clear_kernel<K><<<blocks_for(hsize), kBlock, 0, st>>>(ctx->hash_keys.as<K>(), hsize);
+    ++launch_counter(), hash_insert_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, ctx->hash_keys.as<K>(), ctx->hash_vals.as<int32_t>(),
+        (unsigned long long)(hsize - 1));
     ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
-    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells * n_rows), kBlock, 0, st>>>(ctx->cell_key.as<K>(), n_cells, pl.g, pl.st,
-                                                                  ctx->nbr.as<int2>());
+    int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
+    ck(ctx, cudaMemcpyAsync(rows_dev, pl.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
+    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells * n_rows), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, ctx->hash_keys.as<K>(),
+        ctx->hash_vals.as<int32_t>(), (unsigned long long)(hsize - 1), ctx->nbr.as<int2>());
+    ensure(ctx, ctx->cell_x, (n_cells + 1) * sizeof(int32_t));
+    ++launch_counter(), cell_x_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(ctx->cell_key.as<K>(), n_cells,
+                                                                               pl.g.g[0], ctx->cell_x.as<int32_t>());
     ck(ctx, cudaGetLastError());
 
     // work items
@@ -397,11 +416,16 @@ void labels_phase(ndb_ctx *ctx) {
     const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
     cudaEventRecord(ctx->kev[4], st);
     if (ctx->n_items > 0) {
-        if (ctx->cell_units)
-            ++launch_counter(), union_cells_kernel<D><<<grid, kBlock, 0, st>>>(
-                ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
-                ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                ctx->parent.as<int32_t>(), counters + 3, err);
+        if (ctx->cell_units) {
+            ++launch_counter(), union_cells_kernel<D, true><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
+                n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->n_near_rows,
+                ctx->cell_x.as<int32_t>(), ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(),
+                ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err);
+            ++launch_counter(), union_cells_kernel<D, false><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
+                n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->n_near_rows,
+                ctx->cell_x.as<int32_t>(), ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(),
+                ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err);
+        }
         else
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
@@ -410,11 +434,10 @@ void labels_phase(ndb_ctx *ctx) {
         ck(ctx, cudaGetLastError());
     }
     cudaEventRecord(ctx->kev[5], st);
-    ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(nv, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(),
-                                                       ctx->pcell.as<int32_t>(), ctx->cell_units,
-                                                       ctx->rank.as<uint32_t>(), ctx->parent.as<int32_t>(),
-                                                       ctx->comp_min.as<int32_t>(), err);
     ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units, err);
+    ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+        nv, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units,
+        ctx->rank.as<uint32_t>(), ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>());
     ++launch_counter(), core_ids_kernel<<<blocks_for(n), kBlock, 0, st>>>(
         nv, n, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units,
         ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(), ctx->rank.as<uint32_t>(),
@@ -509,8 +532,9 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->grid = pl.g;
     ctx->stencil = pl.st;
     ctx->n_rows = pl.st.n_rows;
+    ctx->n_near_rows = pl.n_near_rows;
     ctx->cell_units = pl.cell_units ? 1 : 0;
-    if (pl.st.n_rows > kMaxRows) return NDB_ERR_INVALID_ARGUMENT;
+    if (pl.st.n_rows > kWarp) return NDB_ERR_INVALID_ARGUMENT;  // row tables hold one row per lane
 
     classify_dispatch<D>(ctx, pl);
 
@@ -665,7 +689,8 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
                       &ctx->nn_orig,     &ctx->core_sorted, &ctx->core_orig, &ctx->rank,       &ctx->ci_sorted,
                       &ctx->ci_orig,     &ctx->labels,    &ctx->cell_start, &ctx->cell_key,    &ctx->nbr,
                       &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
-                      &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small};
+                      &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small,
+                      &ctx->hash_keys,   &ctx->hash_vals, &ctx->cell_x};
     for (DevBuf *b : bufs) b->release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -812,7 +837,7 @@ enum NaBuf {
     NA_KEYS0, NA_KEYS1, NA_IDS0, NA_IDS1, NA_FLAGS, NA_POS, NA_PCELL, NA_XS, NA_NN_SORTED, NA_NN_ORIG,
     NA_CORE_SORTED, NA_CORE_ORIG, NA_RANK, NA_CI_SORTED, NA_CI_ORIG, NA_LABELS, NA_CELL_START, NA_CELL_KEY,
     NA_NBR, NA_ITEM_CNT, NA_ITEMS, NA_CELL_HAS_CORE, NA_CELL_CID, NA_PARENT, NA_COMP_MIN, NA_SORT_HIST,
-    NA_SCAN, NA_SMALL, NA_COUNT
+    NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_CELL_X, NA_COUNT
 };
 
 constexpr size_t na_cap(int b) {
@@ -825,7 +850,9 @@ constexpr size_t na_cap(int b) {
          : b == NA_CORE_SORTED || b == NA_CELL_HAS_CORE ? kNaN + 1
          : b == NA_SORT_HIST ? 4 * 256 * ((kNaN + kSortTile - 1) / kSortTile)
          : b == NA_SCAN ? 4 * 4096
-         : b == NA_SMALL ? 2048
+         : b == NA_SMALL ? kSmallBytes
+         : b == NA_HASH_KEYS ? 8 * 2 * kNaN
+         : b == NA_HASH_VALS ? 4 * 2 * kNaN
          : 4 * (kNaN + 1);
 }
 
@@ -848,7 +875,8 @@ DevBuf *na_buf(ndb_ctx &c, int b) {
                               &c.core_sorted, &c.core_orig, &c.rank,      &c.ci_sorted,    &c.ci_orig,
                               &c.labels,      &c.cell_start, &c.cell_key, &c.nbr,          &c.item_cnt,
                               &c.items,       &c.cell_has_core, &c.cell_cid, &c.parent,    &c.comp_min,
-                              &c.sort_hist,   &c.scan_scratch, &c.small};
+                              &c.sort_hist,   &c.scan_scratch, &c.small,     &c.hash_keys, &c.hash_vals,
+                              &c.cell_x};
     return bufs[b];
 }
 

@@ -149,8 +149,9 @@ __global__ void __launch_bounds__(kBlock) key_kernel(const float *__restrict__ c
     K key = invalid_key;
     if (point_valid<D>(p)) {
         unsigned long long kk = 0;
-        for (int a = 0; a < g.k; ++a)
-            kk += (unsigned long long)cell_coord(g, a, p[g.dim[a]]) * g.stride[a];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (a < g.k) kk += (unsigned long long)cell_coord(g, a, p[g.dim[a]]) * g.stride[a];
         key = (K)kk;
     }
     keys[i] = key;
@@ -204,51 +205,100 @@ __global__ void __launch_bounds__(kBlock) gather_kernel(const float *__restrict_
     }
 }
 
-template <typename K>
-__device__ __forceinline__ int64_t lower_bound_key(const K *__restrict__ a, int64_t n, unsigned long long key) {
-    int64_t lo = 0, hi = n;
-    while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if ((unsigned long long)__ldg(a + mid) < key) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
+// Open-addressing hash table of the non-empty cells: key -> cell index.  Empty
+// slots hold the all-ones key, which no cell has (it marks invalid points).
+__device__ __forceinline__ unsigned long long hash_slot(unsigned long long key, unsigned long long mask) {
+    return ((key + 1ull) * 0x9E3779B97F4A7C15ull >> 17) & mask;
 }
 
-// nbr[c * n_rows + r] = [first, last) cell index of row r around cell c.
+template <typename K>
+__global__ void hash_clear_kernel(K *__restrict__ hkeys, int64_t size) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < size) hkeys[i] = ~(K)0;
+}
+
+__device__ __forceinline__ uint32_t key_cas(uint32_t *a, uint32_t cmp, uint32_t val) { return atomicCAS(a, cmp, val); }
+__device__ __forceinline__ uint64_t key_cas(uint64_t *a, uint64_t cmp, uint64_t val) {
+    return (uint64_t)atomicCAS(reinterpret_cast<unsigned long long *>(a), (unsigned long long)cmp,
+                               (unsigned long long)val);
+}
+
+template <typename K>
+__global__ void hash_insert_kernel(const K *__restrict__ cell_key, int64_t n_cells, K *hkeys,
+                                   int32_t *__restrict__ hvals, unsigned long long mask) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    const K key = cell_key[c];
+    unsigned long long h = hash_slot((unsigned long long)key, mask);
+    for (unsigned long long probe = 0; probe <= mask; ++probe) {
+        const K prev = key_cas(hkeys + h, ~(K)0, key);
+        if (prev == ~(K)0 || prev == key) {
+            hvals[h] = (int32_t)c;
+            return;
+        }
+        h = (h + 1) & mask;
+    }
+}
+
+template <typename K>
+__device__ __forceinline__ int hash_find(const K *__restrict__ hkeys, const int32_t *__restrict__ hvals,
+                                         unsigned long long mask, unsigned long long key) {
+    unsigned long long h = hash_slot(key, mask);
+    for (unsigned long long probe = 0; probe <= mask; ++probe) {
+        const K k = __ldg(hkeys + h);
+        if ((unsigned long long)k == key) return __ldg(hvals + h);
+        if (k == ~(K)0) return -1;
+        h = (h + 1) & mask;
+    }
+    return -1;
+}
+
+// nbr[c * n_rows + r] = [first, last) cell index of row r around cell c: the cells
+// of a row have consecutive keys, so the existing ones are consecutive in the
+// sorted cell list and the range runs from the smallest to the largest found.
 template <typename K>
 __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell_key, int64_t n_cells,
-                                                      GridDev g, Stencil st, int2 *__restrict__ nbr) {
+                                                      GridDev g, const int4 *__restrict__ rows, int n_rows,
+                                                      const K *__restrict__ hkeys, const int32_t *__restrict__ hvals,
+                                                      unsigned long long mask, int2 *__restrict__ nbr) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n_cells * st.n_rows) return;
-    const int64_t c = idx / st.n_rows;
-    const int r = (int)(idx - c * st.n_rows);
+    if (idx >= n_cells * n_rows) return;
+    const int64_t c = idx / n_rows;
+    const int r = (int)(idx - c * n_rows);
     const unsigned long long key = (unsigned long long)cell_key[c];
-    long long cc[3] = {0, 0, 0};
-    unsigned long long rest = key;
-    for (int a = 0; a < g.k; ++a) {
-        if (a == g.k - 1) {
-            cc[a] = (long long)rest;
-        } else {
-            cc[a] = (long long)(rest % (unsigned long long)g.g[a]);
-            rest /= (unsigned long long)g.g[a];
-        }
-    }
-    const int4 row = st.rows[r];
-    const long long y = cc[1] + row.x, z = cc[2] + row.y;
+    const unsigned long long g0 = (unsigned long long)g.g[0], g1 = (unsigned long long)g.g[1];
+    const long long c0 = (long long)(key % g0);
+    const unsigned long long rest = key / g0;
+    const long long c1 = g.k >= 3 ? (long long)(rest % g1) : (long long)rest;
+    const long long c2 = g.k >= 3 ? (long long)(rest / g1) : 0;
+    const int4 row = __ldg(rows + r);
+    const long long y = c1 + row.x, z = c2 + row.y;
     int2 out = make_int2(0, 0);
     const bool in = (g.k < 2 || (y >= 0 && y < g.g[1])) && (g.k < 3 || (z >= 0 && z < g.g[2]));
     if (in) {
-        const long long x0 = cc[0] - row.z < 0 ? 0 : cc[0] - row.z;
-        const long long x1 = cc[0] + row.z > g.g[0] - 1 ? g.g[0] - 1 : cc[0] + row.z;
+        const long long x0 = c0 - row.z < 0 ? 0 : c0 - row.z;
+        const long long x1 = c0 + row.z > g.g[0] - 1 ? g.g[0] - 1 : c0 + row.z;
         unsigned long long base = 0;
         if (g.k >= 2) base += (unsigned long long)y * g.stride[1];
         if (g.k >= 3) base += (unsigned long long)z * g.stride[2];
-        const int64_t ca = lower_bound_key(cell_key, n_cells, base + (unsigned long long)x0);
-        const int64_t cb = lower_bound_key(cell_key, n_cells, base + (unsigned long long)x1 + 1ull);
-        out = make_int2((int)ca, (int)cb);
+        int lo = 0x7fffffff, hi = -1;
+        for (long long x = x0; x <= x1; ++x) {
+            const int ci = hash_find(hkeys, hvals, mask, base + (unsigned long long)x);
+            if (ci >= 0) {
+                lo = min(lo, ci);
+                hi = max(hi, ci);
+            }
+        }
+        if (hi >= 0) out = make_int2(lo, hi + 1);
     }
     nbr[idx] = out;
+}
+
+template <typename K>
+__global__ void cell_x_kernel(const K *__restrict__ cell_key, int64_t n_cells, long long g0,
+                              int32_t *__restrict__ cell_x) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n_cells) cell_x[c] = (int32_t)((unsigned long long)cell_key[c] % (unsigned long long)g0);
 }
 
 __global__ void item_count_kernel(const int32_t *__restrict__ cell_start, int64_t n_cells,
@@ -269,10 +319,65 @@ __global__ void item_write_kernel(const int32_t *__restrict__ cell_start, int64_
 }
 
 // ---------------------------------------------------------------------------
+// Row table: the candidate ranges of one cell's stencil rows, gathered by the
+// warp in one round (lane r loads row r) and flattened, so that the lanes walk the
+// candidates of all rows 32 at a time instead of row by row.  Host planning keeps
+// the number of rows <= 32.
+// ---------------------------------------------------------------------------
+struct RowTable {
+    int start[kWarp];    // first candidate (point index, or cell index for CELLS) of each row
+    int off[kWarp + 1];  // exclusive prefix of the row lengths; off[n_rows] = total
+};
+
+// CELLS: ranges of cell indices >= min_cell; otherwise ranges of point indices.
+template <bool CELLS>
+__device__ __forceinline__ int gather_rows(const int2 *__restrict__ nbr_row, int n_rows,
+                                           const int32_t *__restrict__ cell_start, int min_cell,
+                                           RowTable &rt, int lane) {
+    int start = 0, len = 0;
+    if (lane < n_rows) {
+        const int2 cr = nbr_row[lane];
+        if (CELLS) {
+            start = max(cr.x, min_cell);
+            len = max(cr.y - start, 0);
+        } else if (cr.x < cr.y) {
+            start = cell_start[cr.x];
+            len = cell_start[cr.y] - start;
+        }
+    }
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane < n_rows) {
+        rt.start[lane] = start;
+        rt.off[lane] = incl - len;
+    }
+    const int total = __shfl_sync(kFull, incl, kWarp - 1);
+    if (lane == 0) rt.off[n_rows] = total;
+    __syncwarp();
+    return total;
+}
+
+// Candidate t (0 <= t < total) of the flattened rows: the last row whose offset is <= t.
+__device__ __forceinline__ int row_lookup(const RowTable &rt, int n_rows, int t) {
+    int lo = 0, hi = n_rows - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (rt.off[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return rt.start[lo] + (t - rt.off[lo]);
+}
+
+// ---------------------------------------------------------------------------
 // Neighbour count.  One warp per item (up to 32 points i of one cell).  The i
-// points sit in shared memory; lanes walk the candidate points j of the
-// stencil rows 32 at a time (coalesced loads), every lane tests its j against
-// each i (broadcast reads) and the warp adds popc(ballot) to that i's count.
+// points sit in shared memory; lanes walk the flattened candidates of the
+// stencil rows 32 at a time (coalesced loads), every lane tests its candidate j
+// against each i (broadcast reads) and the warp adds popc(ballot) to that i's
+// count.  Rows are ordered nearest first.
 // EARLY: stop once every i of the item has reached min_pts (exact counts below
 // min_pts, so exact core flags).  dense_skip: with same-cell-linked cells a cell
 // of >= min_pts points is all cores (every pair inside it is in range), so its
@@ -285,6 +390,7 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     int dense_skip, int32_t *__restrict__ nn_sorted, unsigned long long *__restrict__ pair_counter) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
+    __shared__ RowTable s_rows[kWarpsPerBlock];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     if (item_id >= n_items) return;
@@ -297,47 +403,37 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         return;
     }
     float *si = s_i[wib];
+    RowTable &rt = s_rows[wib];
     if (lane < cnt) {
         float x[D];
         load_point<D>(xs, p0 + lane, x);
         store_point_smem<D>(si + lane * P, x);
     }
-    __syncwarp();
+    const int total = gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, rt, lane);
     int c[kTile];
 #pragma unroll
     for (int k = 0; k < kTile; ++k) c[k] = 0;
     unsigned long long pairs = 0;
-    const int2 *cr = nbr + (int64_t)cell * n_rows;
-    for (int r = 0; r < n_rows; ++r) {
-        const int2 range = cr[r];
-        if (range.x >= range.y) continue;
-        const int j0 = cell_start[range.x], j1 = cell_start[range.y];
-        bool done = false;
-        for (int jb = j0; jb < j1; jb += kWarp) {
-            const int j = jb + lane;
-            float xj[D];
-            if (j < j1) load_point<D>(xs, j, xj);
-            else fill_nan<D>(xj);  // NaN fails the predicate
+    for (int tb = 0; tb < total; tb += kWarp) {
+        const int t = tb + lane;
+        float xj[D];
+        if (t < total) load_point<D>(xs, row_lookup(rt, n_rows, t), xj);
+        else fill_nan<D>(xj);  // NaN fails the predicate
 #pragma unroll
-            for (int k = 0; k < kTile; ++k) {
-                if (k < cnt) {
-                    float xi[D];
-                    load_point_smem<D>(si + k * P, xi);
-                    c[k] += __popc(__ballot_sync(kFull, in_range<D>(xi, xj, e2)));
-                }
-            }
-            pairs += (unsigned long long)cnt * (unsigned long long)min(kWarp, j1 - jb);
-            if (EARLY) {
-                bool all = true;
-#pragma unroll
-                for (int k = 0; k < kTile; ++k) all = all && (k >= cnt || c[k] >= min_pts);
-                if (all) {
-                    done = true;
-                    break;
-                }
+        for (int k = 0; k < kTile; ++k) {
+            if (k < cnt) {
+                float xi[D];
+                load_point_smem<D>(si + k * P, xi);
+                c[k] += __popc(__ballot_sync(kFull, in_range<D>(xi, xj, e2)));
             }
         }
-        if (done) break;
+        pairs += (unsigned long long)cnt * (unsigned long long)min(kWarp, total - tb);
+        if (EARLY) {
+            bool all = true;
+#pragma unroll
+            for (int k = 0; k < kTile; ++k) all = all && (k >= cnt || c[k] >= min_pts);
+            if (all) break;
+        }
     }
     int mine = 0;
 #pragma unroll
@@ -396,67 +492,160 @@ __device__ __forceinline__ int load_item_cores(const float *__restrict__ xs, con
     return __popc(mask);
 }
 
+// Is any core of cell A in range of any core of cell B?  A's cores go through
+// shared memory 32 at a time; lanes hold B's points.  Stops at the first hit.
+template <int D>
+__device__ __forceinline__ bool cells_touch(int A, int B, const int32_t *__restrict__ cell_start,
+                                            const float *__restrict__ xs, const uint8_t *__restrict__ core_sorted,
+                                            float e2, float *si, int lane, unsigned long long &pairs) {
+    constexpr int P = Stride<D>::P;
+    const int a0 = cell_start[A], a1 = cell_start[A + 1];
+    const int b0 = cell_start[B], b1 = cell_start[B + 1];
+    for (int ab = a0; ab < a1; ab += kWarp) {
+        const int i = ab + lane;
+        const bool ok = i < a1 && core_sorted[i];
+        const unsigned mask = __ballot_sync(kFull, ok);
+        if (ok) {
+            float x[D];
+            load_point<D>(xs, i, x);
+            store_point_smem<D>(si + __popc(mask & lanemask_lt()) * P, x);
+        }
+        __syncwarp();
+        const int nc = __popc(mask);
+        if (nc == 0) continue;
+        for (int bb = b0; bb < b1; bb += kWarp) {
+            const int j = bb + lane;
+            float xj[D];
+            if (j < b1 && core_sorted[j]) load_point<D>(xs, j, xj);
+            else fill_nan<D>(xj);
+            bool hit = false;
+            for (int k = 0; k < nc; ++k) {
+                float xi[D];
+                load_point_smem<D>(si + k * P, xi);
+                hit = hit || in_range<D>(xi, xj, e2);
+            }
+            pairs += (unsigned long long)nc * (unsigned long long)min(kWarp, b1 - bb);
+            if (__any_sync(kFull, hit)) return true;
+        }
+        __syncwarp();
+    }
+    return false;
+}
+
 // ---------------------------------------------------------------------------
 // Union-find over cells (same-cell-linked grids): every pair inside a cell is in
 // range, so all cores of a cell belong to one component and the cell is the
-// union-find element.  Each item (cores of one chunk of cell A) looks at the
-// cells B > A of its stencil rows that hold cores and whose root differs from
-// A's, and links A and B as soon as one core pair is in range.
+// union-find element.  One warp per cell A: the lanes gather A's half stencil
+// (cells B > A holding cores), find every B's root in parallel, keep the B whose
+// root differs from A's, then link A and B as soon as one core pair is in range.
 // ---------------------------------------------------------------------------
-template <int D>
+constexpr int kMaxCandCells = 128;
+constexpr int kProbe = 4;  // points of a candidate cell tested by the probe
+
+//
+// Two launches.  NEAR: only the 26 adjacent cells (rows with |o1|,|o2| <= 1, x
+// offset <= 1) and only the lane-parallel probe; in dense regions this links
+// nearly every cell.  Then the full pass: every half-stencil cell, with the roots
+// found after NEAR (so far candidates are mostly filtered before any point test),
+// the probe, and an exhaustive (early-exit) scan for what remains.
+template <int D, bool NEAR>
 __global__ void __launch_bounds__(kBlock) union_cells_kernel(
-    const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
-    const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2,
-    const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core,
-    int32_t *parent, unsigned long long *__restrict__ pair_counter, int *err) {
+    int64_t n_cells, const int32_t *__restrict__ cell_start, const int2 *__restrict__ nbr, int n_rows,
+    int n_near_rows, const int32_t *__restrict__ cell_x, const float *__restrict__ xs, float e2,
+    const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core, int32_t *parent,
+    unsigned long long *__restrict__ pair_counter, int *err) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
-    __shared__ int s_idx[kWarpsPerBlock][kTile];
+    __shared__ RowTable s_rows[kWarpsPerBlock];
+    __shared__ int s_b[kWarpsPerBlock][kMaxCandCells];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
-    if (item_id >= n_items) return;
-    const int2 item = items[item_id];
-    const int A = item.x, p0 = item.y;
+    const int64_t A64 = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    if (A64 >= n_cells) return;
+    const int A = (int)A64;
     if (!cell_has_core[A]) return;
-    const int cnt = min(kTile, cell_start[A + 1] - p0);
-    float *si = s_i[wib];
-    const int nc = load_item_cores<D>(xs, core_sorted, p0, cnt, true, si, s_idx[wib], lane);
-    if (nc == 0) return;
+    RowTable &rt = s_rows[wib];
+    int *sb = s_b[wib];
+    const int rows_used = NEAR ? n_near_rows : n_rows;
+    const int total = gather_rows<true>(nbr + (int64_t)A * n_rows, rows_used, cell_start, A + 1, rt, lane);
+    if (total == 0) return;
+    const int xA = NEAR ? cell_x[A] : 0;
+    int rootA = 0;
+    if (lane == 0) rootA = uf_find(parent, A, err);
+    rootA = __shfl_sync(kFull, rootA, 0);
+    int nb = 0;
+    for (int tb = 0; tb < total; tb += kWarp) {
+        const int t = tb + lane;
+        bool ok = false;
+        int B = 0;
+        if (t < total) {
+            B = row_lookup(rt, rows_used, t);
+            ok = cell_has_core[B] && (!NEAR || abs(cell_x[B] - xA) <= 1) && uf_find(parent, B, err) != rootA;
+        }
+        const unsigned mask = __ballot_sync(kFull, ok);
+        if (ok) {
+            const int slot = nb + __popc(mask & lanemask_lt());
+            if (slot < kMaxCandCells) sb[slot] = B;
+        }
+        nb += __popc(mask);
+    }
+    __syncwarp();
+    nb = min(nb, kMaxCandCells);
     unsigned long long pairs = 0;
-    const int2 *cr = nbr + (int64_t)A * n_rows;
-    for (int r = 0; r < n_rows; ++r) {
-        const int2 range = cr[r];
-        for (int B = max(range.x, A + 1); B < range.y; ++B) {
-            if (!cell_has_core[B]) continue;
-            int same = 0;
-            if (lane == 0) same = uf_find(parent, A, err) == uf_find(parent, B, err);
-            if (__shfl_sync(kFull, same, 0)) continue;
-            const int j0 = cell_start[B], j1 = cell_start[B + 1];
-            bool found = false;
-            for (int jb = j0; jb < j1 && !found; jb += kWarp) {
-                const int j = jb + lane;
+    // Probe: A's first cores go to shared memory; each lane takes one candidate B
+    // and tests B's first kProbe points against them.  Adjacent dense cells are
+    // almost always settled here, in one lane-parallel round.
+    {
+        constexpr int P = Stride<D>::P;
+        float *si = s_i[wib];
+        const int a0 = cell_start[A], a1 = min(cell_start[A + 1], a0 + kWarp);
+        const bool ok = a0 + lane < a1 && core_sorted[a0 + lane];
+        const unsigned mask = __ballot_sync(kFull, ok);
+        if (ok) {
+            float x[D];
+            load_point<D>(xs, a0 + lane, x);
+            store_point_smem<D>(si + __popc(mask & lanemask_lt()) * P, x);
+        }
+        __syncwarp();
+        const int nc0 = __popc(mask);
+        for (int q = lane; q < nb; q += kWarp) {
+            const int B = sb[q];
+            const int b0 = cell_start[B], b1 = min(cell_start[B + 1], b0 + kProbe);
+            bool hit = false;
+            for (int j = b0; j < b1 && !hit; ++j) {
+                if (!core_sorted[j]) continue;
                 float xj[D];
-                if (j < j1 && core_sorted[j]) load_point<D>(xs, j, xj);
-                else fill_nan<D>(xj);
-                bool hit = false;
-                for (int k = 0; k < nc; ++k) {
+                load_point<D>(xs, j, xj);
+                for (int k = 0; k < nc0 && !hit; ++k) {
                     float xi[D];
                     load_point_smem<D>(si + k * P, xi);
-                    hit = hit || in_range<D>(xi, xj, e2);
+                    hit = in_range<D>(xi, xj, e2);
                 }
-                pairs += (unsigned long long)nc * (unsigned long long)min(kWarp, j1 - jb);
-                found = __any_sync(kFull, hit);
+                pairs += (unsigned long long)nc0;
             }
-            if (found && lane == 0) uf_union(parent, A, B, err);
+            if (hit) {
+                uf_union(parent, A, B, err);
+                sb[q] = -1;
+            }
         }
+        __syncwarp();
+    }
+    for (int q = 0; q < (NEAR ? 0 : nb); ++q) {
+        const int B = sb[q];
+        if (B < 0) continue;
+        int same = 0;
+        if (lane == 0) same = uf_find(parent, A, err) == uf_find(parent, B, err);
+        if (__shfl_sync(kFull, same, 0)) continue;
+        if (cells_touch<D>(A, B, cell_start, xs, core_sorted, e2, s_i[wib], lane, pairs) && lane == 0)
+            uf_union(parent, A, B, err);
+        __syncwarp();
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
 }
 
 // ---------------------------------------------------------------------------
-// Union-find over core points (general grids).  Pairs are visited once
-// (j > i in sorted order); a pair whose j already shares i's root is skipped
-// before the predicate.
+// Union-find over core points (general grids).  Pairs are visited once (j > i in
+// sorted order); a pair whose j already shares i's root is skipped before the
+// predicate.
 // ---------------------------------------------------------------------------
 template <int D>
 __global__ void __launch_bounds__(kBlock) union_points_kernel(
@@ -468,6 +657,7 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ int s_idx[kWarpsPerBlock][kTile];
     __shared__ int s_root[kWarpsPerBlock][kTile];
+    __shared__ RowTable s_rows[kWarpsPerBlock];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     if (item_id >= n_items) return;
@@ -478,55 +668,66 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     float *si = s_i[wib];
     int *sidx = s_idx[wib];
     int *sroot = s_root[wib];
+    RowTable &rt = s_rows[wib];
     const int nc = load_item_cores<D>(xs, core_sorted, p0, cnt, true, si, sidx, lane);
     if (nc == 0) return;
+    const int total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
+    if (lane < nc) sroot[lane] = uf_find(parent, sidx[lane], err);
+    __syncwarp();
     unsigned long long pairs = 0;
-    const int2 *cr = nbr + (int64_t)A * n_rows;
-    for (int r = 0; r < n_rows; ++r) {
-        const int2 range = cr[r];
-        if (range.x >= range.y) continue;
-        const int j0 = max(cell_start[range.x], p0 + 1), j1 = cell_start[range.y];
-        if (lane < nc) sroot[lane] = uf_find(parent, sidx[lane], err);
-        __syncwarp();
-        for (int jb = j0; jb < j1; jb += kWarp) {
-            const int j = jb + lane;
-            const bool valid = j < j1 && core_sorted[j];
-            float xj[D];
-            int pj = -1;
-            if (valid) {
-                load_point<D>(xs, j, xj);
-                pj = __ldcg(parent + j);
-            } else {
-                fill_nan<D>(xj);
-            }
-            for (int k = 0; k < nc; ++k) {
-                const int ik = sidx[k];
-                if (valid && j > ik && sroot[k] != pj) {
-                    float xi[D];
-                    load_point_smem<D>(si + k * P, xi);
-                    if (in_range<D>(xi, xj, e2)) {
-                        uf_union(parent, ik, j, err);
-                        pj = uf_find(parent, j, err);
-                    }
+    for (int tb = 0; tb < total; tb += kWarp) {
+        const int t = tb + lane;
+        int j = -1;
+        if (t < total) j = row_lookup(rt, n_rows, t);
+        const bool valid = j > p0 && core_sorted[j];
+        float xj[D];
+        int pj = -1;
+        if (valid) {
+            load_point<D>(xs, j, xj);
+            pj = __ldcg(parent + j);
+        } else {
+            fill_nan<D>(xj);
+        }
+        for (int k = 0; k < nc; ++k) {
+            const int ik = sidx[k];
+            if (valid && j > ik && sroot[k] != pj) {
+                float xi[D];
+                load_point_smem<D>(si + k * P, xi);
+                if (in_range<D>(xi, xj, e2)) {
+                    uf_union(parent, ik, j, err);
+                    pj = uf_find(parent, j, err);
                 }
             }
-            pairs += (unsigned long long)nc * (unsigned long long)min(kWarp, j1 - jb);
         }
-        __syncwarp();
+        pairs += (unsigned long long)nc * (unsigned long long)min(kWarp, total - tb);
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
 }
 
-// comp_min[root] = min core rank in the component
+// comp_min[root] = min core rank in the component.  Runs after flatten_kernel, so
+// parent[u] is the root; lanes that share a root combine their minimum first and
+// one lane per root issues the atomic (clusters have millions of cores).
 __global__ void comp_min_kernel(int64_t nv, const uint8_t *__restrict__ core_sorted,
                                 const int32_t *__restrict__ perm, const int32_t *__restrict__ pcell,
-                                int cell_units, const uint32_t *__restrict__ rank, int32_t *parent,
-                                int32_t *__restrict__ comp_min, int *err) {
+                                int cell_units, const uint32_t *__restrict__ rank, const int32_t *__restrict__ parent,
+                                int32_t *__restrict__ comp_min) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nv || !core_sorted[s]) return;
-    const int u = cell_units ? pcell[s] : (int)s;
-    const int root = uf_find(parent, u, err);
-    atomicMin(comp_min + root, (int32_t)rank[perm[s]]);
+    const bool ok = s < nv && core_sorted[s];
+    int root = -1, r = kNoCluster;
+    if (ok) {
+        root = parent[cell_units ? pcell[s] : (int)s];
+        r = (int)rank[perm[s]];
+    }
+    unsigned pending = __ballot_sync(kFull, ok);
+    const int lane = threadIdx.x & 31;
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const int lroot = __shfl_sync(kFull, root, leader);
+        const bool mine = ok && root == lroot;
+        const int m = (int)__reduce_min_sync(kFull, mine ? (unsigned)r : (unsigned)kNoCluster);
+        if (lane == leader) atomicMin(comp_min + lroot, m);
+        pending &= ~__ballot_sync(kFull, mine);
+    }
 }
 
 __global__ void flatten_kernel(int32_t *parent, int64_t n_units, int *err) {
@@ -593,8 +794,12 @@ __global__ void cell_ids_kernel(int64_t n_cells, const uint8_t *__restrict__ cel
 // ---------------------------------------------------------------------------
 // Border points: every non-core point takes the minimum cluster id over the
 // cores in range (data_process.cpp:204-209), NO_CLUSTER when there is none.
-// With cell units all cores of a cell share one id, so a cell is skipped when
-// its id cannot lower any pending minimum, and its scan stops at the first hit.
+// Cell units: all cores of a cell share one id, so the warp lists the stencil's
+// core cells with their ids, sorts them by id, and walks them in that order; a
+// point is settled by the first cell that has a core in range, and the walk ends
+// once every point of the item is settled or no cell can lower its minimum.
+// Point units: the flattened candidates carry their own ids; the warp takes the
+// minimum over the candidates in range.
 // ---------------------------------------------------------------------------
 template <int D>
 __global__ void __launch_bounds__(kBlock) border_kernel(
@@ -606,6 +811,8 @@ __global__ void __launch_bounds__(kBlock) border_kernel(
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ int s_idx[kWarpsPerBlock][kTile];
+    __shared__ RowTable s_rows[kWarpsPerBlock];
+    __shared__ int2 s_cand[kWarpsPerBlock][kMaxCandCells];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     if (item_id >= n_items) return;
@@ -614,78 +821,124 @@ __global__ void __launch_bounds__(kBlock) border_kernel(
     const int cnt = min(kTile, cell_start[A + 1] - p0);
     float *si = s_i[wib];
     int *sidx = s_idx[wib];
+    RowTable &rt = s_rows[wib];
     const int nb = load_item_cores<D>(xs, core_sorted, p0, cnt, false, si, sidx, lane);
     if (nb == 0) return;
     int best[kTile];
 #pragma unroll
     for (int k = 0; k < kTile; ++k) best[k] = kNoCluster;
     unsigned long long pairs = 0;
-    const int2 *cr = nbr + (int64_t)A * n_rows;
-    for (int r = 0; r < n_rows; ++r) {
-        const int2 range = cr[r];
-        if (range.x >= range.y) continue;
-        if (cell_units) {
-            for (int B = range.x; B < range.y; ++B) {
-                if (!cell_has_core[B]) continue;
-                const int cid = cell_cid[B];
-                bool useful = false;
-#pragma unroll
-                for (int k = 0; k < kTile; ++k) useful = useful || (k < nb && cid < best[k]);
-                if (!useful) continue;
-                const int j0 = cell_start[B], j1 = cell_start[B + 1];
-                for (int jb = j0; jb < j1; jb += kWarp) {
-                    const int j = jb + lane;
-                    float xj[D];
-                    if (j < j1 && core_sorted[j]) load_point<D>(xs, j, xj);
-                    else fill_nan<D>(xj);
-                    bool pending = false;
-#pragma unroll
-                    for (int k = 0; k < kTile; ++k) {
-                        if (k < nb && cid < best[k]) {
-                            float xi[D];
-                            load_point_smem<D>(si + k * P, xi);
-                            if (__any_sync(kFull, in_range<D>(xi, xj, e2))) best[k] = cid;
-                            else pending = true;
-                        }
-                    }
-                    pairs += (unsigned long long)nb * (unsigned long long)min(kWarp, j1 - jb);
-                    if (!pending) break;
-                }
+    if (cell_units) {
+        int2 *cand = s_cand[wib];
+        const int total = gather_rows<true>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
+        int nc = 0;
+        for (int tb = 0; tb < total; tb += kWarp) {
+            const int t = tb + lane;
+            int B = 0;
+            bool ok = false;
+            if (t < total) {
+                B = row_lookup(rt, n_rows, t);
+                ok = cell_has_core[B] != 0;
             }
-        } else {
-            const int j0 = cell_start[range.x], j1 = cell_start[range.y];
+            const unsigned mask = __ballot_sync(kFull, ok);
+            if (ok) {
+                const int slot = nc + __popc(mask & lanemask_lt());
+                if (slot < kMaxCandCells) cand[slot] = make_int2(cell_cid[B], B);
+            }
+            nc += __popc(mask);
+        }
+        __syncwarp();
+        nc = min(nc, kMaxCandCells);
+        // Visit the candidate cells in increasing id order, lazily: each round takes
+        // the smallest remaining id (warp min), and the walk ends once no pending
+        // point can be lowered by it.  Lane l holds candidates l, l+32, ...
+        constexpr int kPer = kMaxCandCells / kWarp;
+        int lcid[kPer];
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int e = q * kWarp + lane;
+            lcid[q] = e < nc ? cand[e].x : kNoCluster;
+        }
+        while (true) {
+            int mloc = kNoCluster, qloc = kPer;
+#pragma unroll
+            for (int q = 0; q < kPer; ++q)
+                if (lcid[q] < mloc) {
+                    mloc = lcid[q];
+                    qloc = q;
+                }
+            const int cid = (int)__reduce_min_sync(kFull, (unsigned)mloc);
+            if (cid == kNoCluster) break;
+            bool useful = false;
+#pragma unroll
+            for (int k = 0; k < kTile; ++k) useful = useful || (k < nb && cid < best[k]);
+            if (!useful) break;  // ids only grow from here
+            const int owner = __ffs(__ballot_sync(kFull, mloc == cid)) - 1;
+            int B = 0;
+            if (lane == owner) {
+#pragma unroll
+                for (int q = 0; q < kPer; ++q)
+                    if (q == qloc) {
+                        B = cand[q * kWarp + lane].y;
+                        lcid[q] = kNoCluster;
+                    }
+            }
+            B = __shfl_sync(kFull, B, owner);
+            const int j0 = cell_start[B], j1 = cell_start[B + 1];
             for (int jb = j0; jb < j1; jb += kWarp) {
                 const int j = jb + lane;
-                const bool valid = j < j1 && core_sorted[j];
                 float xj[D];
-                int cj = kNoCluster;
-                if (valid) {
-                    load_point<D>(xs, j, xj);
-                    cj = ci_sorted[j];
-                } else {
-                    fill_nan<D>(xj);
-                }
+                if (j < j1 && core_sorted[j]) load_point<D>(xs, j, xj);
+                else fill_nan<D>(xj);
+                bool pending = false;
 #pragma unroll
                 for (int k = 0; k < kTile; ++k) {
-                    if (k < nb) {
+                    if (k < nb && cid < best[k]) {
                         float xi[D];
                         load_point_smem<D>(si + k * P, xi);
-                        const int v = (cj < best[k] && in_range<D>(xi, xj, e2)) ? cj : kNoCluster;
-                        best[k] = min(best[k], (int)__reduce_min_sync(kFull, (unsigned)v));
+                        if (__any_sync(kFull, in_range<D>(xi, xj, e2))) best[k] = cid;
+                        else pending = true;
                     }
                 }
                 pairs += (unsigned long long)nb * (unsigned long long)min(kWarp, j1 - jb);
+                if (!pending) break;
             }
         }
+    } else {
+        const int total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
+        for (int tb = 0; tb < total; tb += kWarp) {
+            const int t = tb + lane;
+            int j = -1;
+            if (t < total) j = row_lookup(rt, n_rows, t);
+            const bool valid = j >= 0 && core_sorted[j];
+            float xj[D];
+            int cj = kNoCluster;
+            if (valid) {
+                load_point<D>(xs, j, xj);
+                cj = ci_sorted[j];
+            } else {
+                fill_nan<D>(xj);
+            }
+#pragma unroll
+            for (int k = 0; k < kTile; ++k) {
+                if (k < nb) {
+                    float xi[D];
+                    load_point_smem<D>(si + k * P, xi);
+                    const int v = (cj < best[k] && in_range<D>(xi, xj, e2)) ? cj : kNoCluster;
+                    best[k] = min(best[k], (int)__reduce_min_sync(kFull, (unsigned)v));
+                }
+            }
+            pairs += (unsigned long long)nb * (unsigned long long)min(kWarp, total - tb);
+        }
     }
-    int mine = kNoCluster;
+    int mine_best = kNoCluster;
 #pragma unroll
     for (int k = 0; k < kTile; ++k)
-        if (k == lane) mine = best[k];
+        if (k == lane) mine_best = best[k];
     if (lane < nb) {
         const int s = sidx[lane];
-        ci_sorted[s] = mine;
-        ci_orig[perm[s]] = mine;
+        ci_sorted[s] = mine_best;
+        ci_orig[perm[s]] = mine_best;
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
 }
