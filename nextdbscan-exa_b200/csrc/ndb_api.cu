@@ -417,14 +417,16 @@ void labels_phase(ndb_ctx *ctx) {
     cudaEventRecord(ctx->kev[4], st);
     if (ctx->n_items > 0) {
         if (ctx->cell_units) {
-            ++launch_counter(), union_cells_kernel<D, true><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
+            ++launch_counter(), union_near_kernel<D><<<blocks_for(n_cells * ctx->n_near_rows), kBlock, 0, st>>>(
                 n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->n_near_rows,
                 ctx->cell_x.as<int32_t>(), ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(),
                 ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err);
-            ++launch_counter(), union_cells_kernel<D, false><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
-                n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->n_near_rows,
-                ctx->cell_x.as<int32_t>(), ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(),
-                ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err);
+            ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
+                                                                                      n_units, err);
+            ++launch_counter(), union_cells_kernel<D><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
+                n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->xs.as<float>(),
+                ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
+                counters + 3, err);
         }
         else
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(

@@ -533,6 +533,62 @@ __device__ __forceinline__ bool cells_touch(int A, int B, const int32_t *__restr
 }
 
 // ---------------------------------------------------------------------------
+// First union pass over cells: one thread per (cell A, near stencil row).  The
+// thread looks at the cells B > A of that row that are adjacent to A (|dx| <= 1;
+// near rows have |o1|, |o2| <= 1), tests the first kNearProbe cores of A against
+// the first kNearProbe cores of B (independent loads, 16 predicates) and links A
+// and B on a hit.  Adjacent cells of a dense region are almost always linked here,
+// with far more parallelism than a warp per cell gives.
+// ---------------------------------------------------------------------------
+constexpr int kNearProbe = 4;
+
+template <int D>
+__device__ __forceinline__ void load_first_cores(const float *__restrict__ xs, const uint8_t *__restrict__ core_sorted,
+                                                 int c0, int c1, float (&x)[kNearProbe][D]) {
+#pragma unroll
+    for (int q = 0; q < kNearProbe; ++q) {
+        const int i = c0 + q;
+        if (i < c1 && core_sorted[i]) load_point<D>(xs, i, x[q]);
+        else fill_nan<D>(x[q]);
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kBlock) union_near_kernel(
+    int64_t n_cells, const int32_t *__restrict__ cell_start, const int2 *__restrict__ nbr, int n_rows,
+    int n_near_rows, const int32_t *__restrict__ cell_x, const float *__restrict__ xs, float e2,
+    const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core, int32_t *parent,
+    unsigned long long *__restrict__ pair_counter, int *err) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long pairs = 0;
+    if (idx < n_cells * n_near_rows) {
+        const int A = (int)(idx / n_near_rows);
+        const int r = (int)(idx - (int64_t)A * n_near_rows);
+        const int2 cr = nbr[(int64_t)A * n_rows + r];
+        const int lo = max(cr.x, A + 1);
+        if (lo < cr.y && cell_has_core[A]) {
+            const int xA = cell_x[A];
+            float xa[kNearProbe][D];
+            load_first_cores<D>(xs, core_sorted, cell_start[A], cell_start[A + 1], xa);
+            for (int B = lo; B < cr.y; ++B) {
+                if (abs(cell_x[B] - xA) > 1 || !cell_has_core[B]) continue;
+                float xb[kNearProbe][D];
+                load_first_cores<D>(xs, core_sorted, cell_start[B], cell_start[B + 1], xb);
+                bool hit = false;
+#pragma unroll
+                for (int p = 0; p < kNearProbe; ++p)
+#pragma unroll
+                    for (int q = 0; q < kNearProbe; ++q) hit = hit || in_range<D>(xa[p], xb[q], e2);
+                pairs += kNearProbe * kNearProbe;
+                if (hit) uf_union(parent, A, B, err);
+            }
+        }
+    }
+    pairs = __reduce_add_sync(kFull, (unsigned)pairs);
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(pair_counter, pairs);
+}
+
+// ---------------------------------------------------------------------------
 // Union-find over cells (same-cell-linked grids): every pair inside a cell is in
 // range, so all cores of a cell belong to one component and the cell is the
 // union-find element.  One warp per cell A: the lanes gather A's half stencil
@@ -543,17 +599,14 @@ constexpr int kMaxCandCells = 128;
 constexpr int kProbe = 4;  // points of a candidate cell tested by the probe
 
 //
-// Two launches.  NEAR: only the 26 adjacent cells (rows with |o1|,|o2| <= 1, x
-// offset <= 1) and only the lane-parallel probe; in dense regions this links
-// nearly every cell.  Then the full pass: every half-stencil cell, with the roots
-// found after NEAR (so far candidates are mostly filtered before any point test),
-// the probe, and an exhaustive (early-exit) scan for what remains.
-template <int D, bool NEAR>
+// Runs after union_near_kernel has linked the adjacent dense cells, so the root
+// filter removes most candidates before any point test.
+template <int D>
 __global__ void __launch_bounds__(kBlock) union_cells_kernel(
     int64_t n_cells, const int32_t *__restrict__ cell_start, const int2 *__restrict__ nbr, int n_rows,
-    int n_near_rows, const int32_t *__restrict__ cell_x, const float *__restrict__ xs, float e2,
-    const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core, int32_t *parent,
-    unsigned long long *__restrict__ pair_counter, int *err) {
+    const float *__restrict__ xs, float e2, const uint8_t *__restrict__ core_sorted,
+    const uint8_t *__restrict__ cell_has_core, int32_t *parent, unsigned long long *__restrict__ pair_counter,
+    int *err) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ RowTable s_rows[kWarpsPerBlock];
@@ -565,10 +618,8 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
     if (!cell_has_core[A]) return;
     RowTable &rt = s_rows[wib];
     int *sb = s_b[wib];
-    const int rows_used = NEAR ? n_near_rows : n_rows;
-    const int total = gather_rows<true>(nbr + (int64_t)A * n_rows, rows_used, cell_start, A + 1, rt, lane);
+    const int total = gather_rows<true>(nbr + (int64_t)A * n_rows, n_rows, cell_start, A + 1, rt, lane);
     if (total == 0) return;
-    const int xA = NEAR ? cell_x[A] : 0;
     int rootA = 0;
     if (lane == 0) rootA = uf_find(parent, A, err);
     rootA = __shfl_sync(kFull, rootA, 0);
@@ -578,8 +629,8 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
         bool ok = false;
         int B = 0;
         if (t < total) {
-            B = row_lookup(rt, rows_used, t);
-            ok = cell_has_core[B] && (!NEAR || abs(cell_x[B] - xA) <= 1) && uf_find(parent, B, err) != rootA;
+            B = row_lookup(rt, n_rows, t);
+            ok = cell_has_core[B] && uf_find(parent, B, err) != rootA;
         }
         const unsigned mask = __ballot_sync(kFull, ok);
         if (ok) {
@@ -629,7 +680,7 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
         }
         __syncwarp();
     }
-    for (int q = 0; q < (NEAR ? 0 : nb); ++q) {
+    for (int q = 0; q < nb; ++q) {
         const int B = sb[q];
         if (B < 0) continue;
         int same = 0;
