@@ -26,7 +26,7 @@ struct ndb_ctx {
     DevBuf coords, keys0, keys1, ids0, ids1, flags, pos, pcell, xs;
     DevBuf nn_sorted, nn_orig, core_sorted, core_orig, rank, ci_sorted, ci_orig, labels;
     // per-cell arrays
-    DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid, hash_keys, hash_vals, cell_x;
+    DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid, hash_keys, hash_vals;
     // union-find
     DevBuf parent, comp_min;
     // scratch
@@ -46,7 +46,7 @@ struct ndb_ctx {
     bool key64 = false;
     int cell_units = 0;
     int n_rows = 0;
-    int n_near_rows = 0;
+    unsigned long long hash_mask = 0;
     const float *coords_dev = nullptr;  // device coordinates of the current job
     GridDev grid{};
     Stencil stencil{};
@@ -114,7 +114,6 @@ struct Plan {
     Stencil st{};
     bool cell_units = false;
     int key_bits = 0;
-    int n_near_rows = 0;  // leading rows whose cells are all adjacent in dimensions 1, 2 (|o1|, |o2| <= 1)
 };
 
 Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
@@ -215,10 +214,8 @@ Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
         return std::abs(x.o1) + std::abs(x.o2) < std::abs(y.o1) + std::abs(y.o2);
     });
     pl.st.n_rows = (int)rows.size();
-    for (size_t i = 0; i < rows.size() && i < (size_t)kMaxRows; ++i) {
+    for (size_t i = 0; i < rows.size() && i < (size_t)kMaxRows; ++i)
         pl.st.rows[i] = make_int4(rows[i].o1, rows[i].o2, rows[i].xr, 0);
-        if (std::abs(rows[i].o1) <= 1 && std::abs(rows[i].o2) <= 1 && (int)i == pl.n_near_rows) ++pl.n_near_rows;
-    }
     return pl;
 }
 
@@ -300,6 +297,7 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     const int n_rows = pl.st.n_rows;
     int64_t hsize = 1024;
     while (hsize < 2 * n_cells) hsize <<= 1;
+    ctx->hash_mask = (unsigned long long)(hsize - 1);
     ensure(ctx, ctx->hash_keys, hsize * sizeof(K));
     ensure(ctx, ctx->hash_vals, hsize * sizeof(int32_t));
     ++launch_counter(), hash_clear_kernel<K><<<blocks_for(hsize), kBlock, 0, st>>>(ctx->hash_keys.as<K>(), hsize);
@@ -312,9 +310,6 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells * n_rows), kBlock, 0, st>>>(
         ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, ctx->hash_keys.as<K>(),
         ctx->hash_vals.as<int32_t>(), (unsigned long long)(hsize - 1), ctx->nbr.as<int2>());
-    ensure(ctx, ctx->cell_x, (n_cells + 1) * sizeof(int32_t));
-    ++launch_counter(), cell_x_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(ctx->cell_key.as<K>(), n_cells,
-                                                                               pl.g.g[0], ctx->cell_x.as<int32_t>());
     ck(ctx, cudaGetLastError());
 
     // work items
@@ -417,10 +412,18 @@ void labels_phase(ndb_ctx *ctx) {
     cudaEventRecord(ctx->kev[4], st);
     if (ctx->n_items > 0) {
         if (ctx->cell_units) {
-            ++launch_counter(), union_near_kernel<D><<<blocks_for(n_cells * ctx->n_near_rows), kBlock, 0, st>>>(
-                n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->n_near_rows,
-                ctx->cell_x.as<int32_t>(), ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(),
-                ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err);
+            if (ctx->key64)
+                ++launch_counter(), union_near_kernel<D, uint64_t><<<blocks_for(n_cells), kBlock, 0, st>>>(
+                    n_cells, ctx->grid, ctx->cell_key.as<uint64_t>(), ctx->cell_start.as<int32_t>(),
+                    ctx->hash_keys.as<uint64_t>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask, ctx->xs.as<float>(),
+                    ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+                    ctx->parent.as<int32_t>(), counters + 3, err);
+            else
+                ++launch_counter(), union_near_kernel<D, uint32_t><<<blocks_for(n_cells), kBlock, 0, st>>>(
+                    n_cells, ctx->grid, ctx->cell_key.as<uint32_t>(), ctx->cell_start.as<int32_t>(),
+                    ctx->hash_keys.as<uint32_t>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask, ctx->xs.as<float>(),
+                    ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+                    ctx->parent.as<int32_t>(), counters + 3, err);
             ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                       n_units, err);
             ++launch_counter(), union_cells_kernel<D><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
@@ -534,7 +537,6 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->grid = pl.g;
     ctx->stencil = pl.st;
     ctx->n_rows = pl.st.n_rows;
-    ctx->n_near_rows = pl.n_near_rows;
     ctx->cell_units = pl.cell_units ? 1 : 0;
     if (pl.st.n_rows > kWarp) return NDB_ERR_INVALID_ARGUMENT;  // row tables hold one row per lane
 
@@ -692,7 +694,7 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
                       &ctx->ci_orig,     &ctx->labels,    &ctx->cell_start, &ctx->cell_key,    &ctx->nbr,
                       &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
                       &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small,
-                      &ctx->hash_keys,   &ctx->hash_vals, &ctx->cell_x};
+                      &ctx->hash_keys,   &ctx->hash_vals};
     for (DevBuf *b : bufs) b->release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -839,7 +841,7 @@ enum NaBuf {
     NA_KEYS0, NA_KEYS1, NA_IDS0, NA_IDS1, NA_FLAGS, NA_POS, NA_PCELL, NA_XS, NA_NN_SORTED, NA_NN_ORIG,
     NA_CORE_SORTED, NA_CORE_ORIG, NA_RANK, NA_CI_SORTED, NA_CI_ORIG, NA_LABELS, NA_CELL_START, NA_CELL_KEY,
     NA_NBR, NA_ITEM_CNT, NA_ITEMS, NA_CELL_HAS_CORE, NA_CELL_CID, NA_PARENT, NA_COMP_MIN, NA_SORT_HIST,
-    NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_CELL_X, NA_COUNT
+    NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_COUNT
 };
 
 constexpr size_t na_cap(int b) {
@@ -877,8 +879,7 @@ DevBuf *na_buf(ndb_ctx &c, int b) {
                               &c.core_sorted, &c.core_orig, &c.rank,      &c.ci_sorted,    &c.ci_orig,
                               &c.labels,      &c.cell_start, &c.cell_key, &c.nbr,          &c.item_cnt,
                               &c.items,       &c.cell_has_core, &c.cell_cid, &c.parent,    &c.comp_min,
-                              &c.sort_hist,   &c.scan_scratch, &c.small,     &c.hash_keys, &c.hash_vals,
-                              &c.cell_x};
+                              &c.sort_hist,   &c.scan_scratch, &c.small,     &c.hash_keys, &c.hash_vals};
     return bufs[b];
 }
 

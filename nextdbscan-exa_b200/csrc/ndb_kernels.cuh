@@ -44,6 +44,7 @@ struct Stencil {
 };
 
 constexpr int kBlock = 256;
+constexpr int kMaxRowCells = 5;  // cells per stencil row looked up together (2*xr+1 <= 5)
 constexpr int kWarpsPerBlock = kBlock / kWarp;
 
 // ---------------------------------------------------------------------------
@@ -282,8 +283,28 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
         if (g.k >= 2) base += (unsigned long long)y * g.stride[1];
         if (g.k >= 3) base += (unsigned long long)z * g.stride[2];
         int lo = 0x7fffffff, hi = -1;
-        for (long long x = x0; x <= x1; ++x) {
-            const int ci = hash_find(hkeys, hvals, mask, base + (unsigned long long)x);
+        // first probes of all (at most kMaxRowCells) cells of the row issued together
+        unsigned long long slot[kMaxRowCells];
+        K seen[kMaxRowCells];
+#pragma unroll
+        for (int q = 0; q < kMaxRowCells; ++q) {
+            slot[q] = hash_slot(base + (unsigned long long)(x0 + q), mask);
+            seen[q] = (x0 + q <= x1) ? __ldg(hkeys + slot[q]) : ~(K)0;
+        }
+#pragma unroll
+        for (int q = 0; q < kMaxRowCells; ++q) {
+            if (x0 + q > x1) continue;
+            const unsigned long long want = base + (unsigned long long)(x0 + q);
+            int ci = -1;
+            if ((unsigned long long)seen[q] == want) ci = __ldg(hvals + slot[q]);
+            else if (seen[q] != ~(K)0) ci = hash_find(hkeys, hvals, mask, want);
+            if (ci >= 0) {
+                lo = min(lo, ci);
+                hi = max(hi, ci);
+            }
+        }
+        for (long long xx = x0 + kMaxRowCells; xx <= x1; ++xx) {
+            const int ci = hash_find(hkeys, hvals, mask, base + (unsigned long long)xx);
             if (ci >= 0) {
                 lo = min(lo, ci);
                 hi = max(hi, ci);
@@ -292,13 +313,6 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
         if (hi >= 0) out = make_int2(lo, hi + 1);
     }
     nbr[idx] = out;
-}
-
-template <typename K>
-__global__ void cell_x_kernel(const K *__restrict__ cell_key, int64_t n_cells, long long g0,
-                              int32_t *__restrict__ cell_x) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n_cells) cell_x[c] = (int32_t)((unsigned long long)cell_key[c] % (unsigned long long)g0);
 }
 
 __global__ void item_count_kernel(const int32_t *__restrict__ cell_start, int64_t n_cells,
@@ -533,12 +547,13 @@ __device__ __forceinline__ bool cells_touch(int A, int B, const int32_t *__restr
 }
 
 // ---------------------------------------------------------------------------
-// First union pass over cells: one thread per (cell A, near stencil row).  The
-// thread looks at the cells B > A of that row that are adjacent to A (|dx| <= 1;
-// near rows have |o1|, |o2| <= 1), tests the first kNearProbe cores of A against
-// the first kNearProbe cores of B (independent loads, 16 predicates) and links A
-// and B on a hit.  Adjacent cells of a dense region are almost always linked here,
-// with far more parallelism than a warp per cell gives.
+// First union pass over cells: one thread per cell A.  It looks at A's three
+// forward face neighbours (x+1, y+1, z+1; found through the key order and the cell
+// hash table), tests the first kNearProbe cores of A against the first
+// kNearProbe cores of each (independent loads, 16 predicates) and links A and B on
+// a hit.  Face adjacency already connects every cell of a dense region, so this
+// merges dense clusters with one cheap thread per cell; the full pass then sees
+// them as one root.
 // ---------------------------------------------------------------------------
 constexpr int kNearProbe = 4;
 
@@ -553,25 +568,40 @@ __device__ __forceinline__ void load_first_cores(const float *__restrict__ xs, c
     }
 }
 
-template <int D>
+template <int D, typename K>
 __global__ void __launch_bounds__(kBlock) union_near_kernel(
-    int64_t n_cells, const int32_t *__restrict__ cell_start, const int2 *__restrict__ nbr, int n_rows,
-    int n_near_rows, const int32_t *__restrict__ cell_x, const float *__restrict__ xs, float e2,
-    const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core, int32_t *parent,
-    unsigned long long *__restrict__ pair_counter, int *err) {
+    int64_t n_cells, GridDev g, const K *__restrict__ cell_key, const int32_t *__restrict__ cell_start,
+    const K *__restrict__ hkeys, const int32_t *__restrict__ hvals, unsigned long long mask,
+    const float *__restrict__ xs, float e2, const uint8_t *__restrict__ core_sorted,
+    const uint8_t *__restrict__ cell_has_core, int32_t *parent, unsigned long long *__restrict__ pair_counter,
+    int *err) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long pairs = 0;
-    if (idx < n_cells * n_near_rows) {
-        const int A = (int)(idx / n_near_rows);
-        const int r = (int)(idx - (int64_t)A * n_near_rows);
-        const int2 cr = nbr[(int64_t)A * n_rows + r];
-        const int lo = max(cr.x, A + 1);
-        if (lo < cr.y && cell_has_core[A]) {
-            const int xA = cell_x[A];
+    unsigned pairs = 0;
+    if (idx < n_cells && cell_has_core[idx]) {
+        const int A = (int)idx;
+        const unsigned long long key = (unsigned long long)cell_key[A];
+        const unsigned long long g0 = (unsigned long long)g.g[0], g1 = (unsigned long long)g.g[1];
+        const unsigned long long rest = key / g0;
+        const long long x = (long long)(key - rest * g0);
+        const long long y = g.k >= 3 ? (long long)(rest % g1) : (long long)rest;
+        const long long z = g.k >= 3 ? (long long)(rest / g1) : 0;
+        int nb[3] = {-1, -1, -1};
+        if (x + 1 < g.g[0] && A + 1 < n_cells && (unsigned long long)cell_key[A + 1] == key + 1ull) nb[0] = A + 1;
+        if (g.k >= 2 && y + 1 < g.g[1]) nb[1] = hash_find(hkeys, hvals, mask, key + g.stride[1]);
+        if (g.k >= 3 && z + 1 < g.g[2]) nb[2] = hash_find(hkeys, hvals, mask, key + g.stride[2]);
+        bool any = false;
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            if (nb[f] >= 0 && !cell_has_core[nb[f]]) nb[f] = -1;
+            any = any || nb[f] >= 0;
+        }
+        if (any) {
             float xa[kNearProbe][D];
             load_first_cores<D>(xs, core_sorted, cell_start[A], cell_start[A + 1], xa);
-            for (int B = lo; B < cr.y; ++B) {
-                if (abs(cell_x[B] - xA) > 1 || !cell_has_core[B]) continue;
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                if (nb[f] < 0) continue;
+                const int B = nb[f];
                 float xb[kNearProbe][D];
                 load_first_cores<D>(xs, core_sorted, cell_start[B], cell_start[B + 1], xb);
                 bool hit = false;
@@ -584,8 +614,8 @@ __global__ void __launch_bounds__(kBlock) union_near_kernel(
             }
         }
     }
-    pairs = __reduce_add_sync(kFull, (unsigned)pairs);
-    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(pair_counter, pairs);
+    pairs = __reduce_add_sync(kFull, pairs);
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(pair_counter, (unsigned long long)pairs);
 }
 
 // ---------------------------------------------------------------------------
