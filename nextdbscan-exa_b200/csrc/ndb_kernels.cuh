@@ -433,15 +433,18 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         float xj[D];
         if (t < total) load_point<D>(xs, row_lookup(rt, n_rows, t), xj);
         else fill_nan<D>(xj);  // NaN fails the predicate
+        int active = 0;
 #pragma unroll
         for (int k = 0; k < kTile; ++k) {
-            if (k < cnt) {
+            // a point that already reached min_pts (EARLY) needs no more tests
+            if (k < cnt && (!EARLY || c[k] < min_pts)) {
                 float xi[D];
                 load_point_smem<D>(si + k * P, xi);
                 c[k] += __popc(__ballot_sync(kFull, in_range<D>(xi, xj, e2)));
+                ++active;
             }
         }
-        pairs += (unsigned long long)cnt * (unsigned long long)min(kWarp, total - tb);
+        pairs += (unsigned long long)active * (unsigned long long)min(kWarp, total - tb);
         if (EARLY) {
             bool all = true;
 #pragma unroll
@@ -753,10 +756,12 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     const int nc = load_item_cores<D>(xs, core_sorted, p0, cnt, true, si, sidx, lane);
     if (nc == 0) return;
     const int total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
-    if (lane < nc) sroot[lane] = uf_find(parent, sidx[lane], err);
-    __syncwarp();
     unsigned long long pairs = 0;
     for (int tb = 0; tb < total; tb += kWarp) {
+        // roots of the item's cores, refreshed every chunk so that candidates already
+        // joined to them are skipped before the predicate
+        if (lane < nc) sroot[lane] = uf_find(parent, sidx[lane], err);
+        __syncwarp();
         const int t = tb + lane;
         int j = -1;
         if (t < total) j = row_lookup(rt, n_rows, t);
@@ -766,21 +771,25 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
         if (valid) {
             load_point<D>(xs, j, xj);
             pj = __ldcg(parent + j);
+            pj = __ldcg(parent + pj);  // two hops: an ancestor of j, usually its root
         } else {
             fill_nan<D>(xj);
         }
+        int tested = 0;
         for (int k = 0; k < nc; ++k) {
             const int ik = sidx[k];
             if (valid && j > ik && sroot[k] != pj) {
                 float xi[D];
                 load_point_smem<D>(si + k * P, xi);
+                ++tested;
                 if (in_range<D>(xi, xj, e2)) {
                     uf_union(parent, ik, j, err);
                     pj = uf_find(parent, j, err);
                 }
             }
         }
-        pairs += (unsigned long long)nc * (unsigned long long)min(kWarp, total - tb);
+        pairs += (unsigned long long)__reduce_add_sync(kFull, (unsigned)tested);
+        __syncwarp();
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
 }
