@@ -29,6 +29,10 @@ struct ndb_ctx {
     DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid, hash_keys, hash_vals;
     // union-find
     DevBuf parent, comp_min;
+    // neighbour lists of the points whose count stays below min_pts (border step)
+    DevBuf nbr_list;
+    size_t list_budget = size_t(8) << 30;  // largest list buffer the context may use (else: scan border)
+    int list_cap = 0;                 // entries per point, 0 when the lists are off
     // scratch
     DevBuf sort_hist, scan_scratch, small;  // small: counters, bbox, scalars
 
@@ -336,16 +340,26 @@ void count_phase(ndb_ctx *ctx) {
     ensure(ctx, ctx->nn_sorted, (ctx->n + 1) * sizeof(int32_t));
     const bool early = (ctx->flags_run & NDB_FLAG_FULL_COUNT) == 0;
     const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    // neighbour lists for the border step: min_pts - 1 entries per point
+    ctx->list_cap = 0;
+    const int64_t cap = (int64_t)ctx->min_pts - 1;
+    if (cap >= 1 && cap <= kMaxListCap && (size_t)(ctx->nv * cap) * sizeof(int32_t) <= ctx->list_budget) {
+        ensure(ctx, ctx->nbr_list, (size_t)(ctx->nv * cap + 1) * sizeof(int32_t));
+        ctx->list_cap = (int)cap;
+    }
+    int32_t *list = ctx->list_cap ? ctx->nbr_list.as<int32_t>() : nullptr;
     cudaEventRecord(ctx->kev[2], st);
     if (ctx->n_items > 0) {
         if (early)
             ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
-                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), counters + 2);
+                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
+                ctx->list_cap, counters + 2);
         else
             ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
-                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), counters + 2);
+                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
+                ctx->list_cap, counters + 2);
         ck(ctx, cudaGetLastError());
     }
     cudaEventRecord(ctx->kev[3], st);
@@ -454,7 +468,13 @@ void labels_phase(ndb_ctx *ctx) {
     ck(ctx, cudaGetLastError());
     cudaEventRecord(ctx->ev[3], st);
     cudaEventRecord(ctx->kev[6], st);
-    if (ctx->n_items > 0) {
+    if (ctx->list_cap > 0) {
+        ++launch_counter(), border_list_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+            nv, ctx->nn_sorted.as<int32_t>(), ctx->nbr_list.as<int32_t>(), ctx->list_cap,
+            ctx->core_sorted.as<uint8_t>(), ctx->cell_units, ctx->pcell.as<int32_t>(), ctx->cell_cid.as<int32_t>(),
+            ctx->ids0.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), ctx->ci_orig.as<int32_t>(), counters + 4);
+        ck(ctx, cudaGetLastError());
+    } else if (ctx->n_items > 0) {
         ++launch_counter(), border_kernel<D><<<grid, kBlock, 0, st>>>(
             ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
             ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
@@ -694,7 +714,7 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
                       &ctx->ci_orig,     &ctx->labels,    &ctx->cell_start, &ctx->cell_key,    &ctx->nbr,
                       &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
                       &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small,
-                      &ctx->hash_keys,   &ctx->hash_vals};
+                      &ctx->hash_keys,   &ctx->hash_vals, &ctx->nbr_list};
     for (DevBuf *b : bufs) b->release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -841,7 +861,7 @@ enum NaBuf {
     NA_KEYS0, NA_KEYS1, NA_IDS0, NA_IDS1, NA_FLAGS, NA_POS, NA_PCELL, NA_XS, NA_NN_SORTED, NA_NN_ORIG,
     NA_CORE_SORTED, NA_CORE_ORIG, NA_RANK, NA_CI_SORTED, NA_CI_ORIG, NA_LABELS, NA_CELL_START, NA_CELL_KEY,
     NA_NBR, NA_ITEM_CNT, NA_ITEMS, NA_CELL_HAS_CORE, NA_CELL_CID, NA_PARENT, NA_COMP_MIN, NA_SORT_HIST,
-    NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_COUNT
+    NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_NBR_LIST, NA_COUNT
 };
 
 constexpr size_t na_cap(int b) {
@@ -857,6 +877,7 @@ constexpr size_t na_cap(int b) {
          : b == NA_SMALL ? kSmallBytes
          : b == NA_HASH_KEYS ? 8 * 2 * kNaN
          : b == NA_HASH_VALS ? 4 * 2 * kNaN
+         : b == NA_NBR_LIST ? 4 * 16 * kNaN
          : 4 * (kNaN + 1);
 }
 
@@ -879,7 +900,8 @@ DevBuf *na_buf(ndb_ctx &c, int b) {
                               &c.core_sorted, &c.core_orig, &c.rank,      &c.ci_sorted,    &c.ci_orig,
                               &c.labels,      &c.cell_start, &c.cell_key, &c.nbr,          &c.item_cnt,
                               &c.items,       &c.cell_has_core, &c.cell_cid, &c.parent,    &c.comp_min,
-                              &c.sort_hist,   &c.scan_scratch, &c.small,     &c.hash_keys, &c.hash_vals};
+                              &c.sort_hist,   &c.scan_scratch, &c.small,     &c.hash_keys, &c.hash_vals,
+                              &c.nbr_list};
     return bufs[b];
 }
 
@@ -938,6 +960,7 @@ extern "C" ndb_status ndb_b200_run_noalloc(const float *coords, int64_t n, int32
         s.ready = true;
     }
     na_carve(s);
+    s.ctx.list_budget = na_cap(NA_NBR_LIST) - 4;  // lists only where they fit the slice
     s.ctx.own_stream = nullptr;
     s.ctx.stream = static_cast<cudaStream_t>(cuda_stream);
     ndb_status st = ndb_b200_classify(&s.ctx, coords, n, d, eps, min_pts, flags | NDB_FLAG_DEVICE_PTRS, nn_out);

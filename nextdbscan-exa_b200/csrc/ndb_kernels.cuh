@@ -44,7 +44,8 @@ struct Stencil {
 };
 
 constexpr int kBlock = 256;
-constexpr int kMaxRowCells = 5;  // cells per stencil row looked up together (2*xr+1 <= 5)
+constexpr int kMaxRowCells = 5;
+constexpr int kMaxListCap = 64;  // largest min_pts - 1 for which neighbour lists are kept  // cells per stencil row looked up together (2*xr+1 <= 5)
 constexpr int kWarpsPerBlock = kBlock / kWarp;
 
 // ---------------------------------------------------------------------------
@@ -401,7 +402,8 @@ template <int D, bool EARLY>
 __global__ void __launch_bounds__(kBlock) count_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts,
-    int dense_skip, int32_t *__restrict__ nn_sorted, unsigned long long *__restrict__ pair_counter) {
+    int dense_skip, int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap,
+    unsigned long long *__restrict__ pair_counter) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ RowTable s_rows[kWarpsPerBlock];
@@ -430,8 +432,9 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     unsigned long long pairs = 0;
     for (int tb = 0; tb < total; tb += kWarp) {
         const int t = tb + lane;
+        const int j = t < total ? row_lookup(rt, n_rows, t) : -1;
         float xj[D];
-        if (t < total) load_point<D>(xs, row_lookup(rt, n_rows, t), xj);
+        if (j >= 0) load_point<D>(xs, j, xj);
         else fill_nan<D>(xj);  // NaN fails the predicate
         int active = 0;
 #pragma unroll
@@ -440,7 +443,15 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
             if (k < cnt && (!EARLY || c[k] < min_pts)) {
                 float xi[D];
                 load_point_smem<D>(si + k * P, xi);
-                c[k] += __popc(__ballot_sync(kFull, in_range<D>(xi, xj, e2)));
+                const bool hit = in_range<D>(xi, xj, e2);
+                const unsigned m = __ballot_sync(kFull, hit);
+                // the first list_cap neighbours of each point; complete for every point
+                // whose count stays below min_pts (list_cap = min_pts - 1)
+                if (nbr_list && m && c[k] < list_cap) {
+                    const int slot = c[k] + __popc(m & lanemask_lt());
+                    if (hit && slot < list_cap) nbr_list[(int64_t)(p0 + k) * list_cap + slot] = j;
+                }
+                c[k] += __popc(m);
                 ++active;
             }
         }
@@ -1031,6 +1042,34 @@ __global__ void __launch_bounds__(kBlock) border_kernel(
         ci_orig[perm[s]] = mine_best;
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
+}
+
+// ---------------------------------------------------------------------------
+// Border points from the count's neighbour lists: a non-core point has fewer than
+// min_pts points in range, all of them recorded by count_kernel, so its id is the
+// minimum id over the cores among them -- no second stencil scan.
+// ---------------------------------------------------------------------------
+__global__ void border_list_kernel(int64_t nv, const int32_t *__restrict__ nn_sorted,
+                                   const int32_t *__restrict__ nbr_list, int list_cap,
+                                   const uint8_t *__restrict__ core_sorted, int cell_units,
+                                   const int32_t *__restrict__ pcell, const int32_t *__restrict__ cell_cid,
+                                   const int32_t *__restrict__ perm, int32_t *__restrict__ ci_sorted,
+                                   int32_t *__restrict__ ci_orig, unsigned long long *__restrict__ pair_counter) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned looked = 0;
+    if (s < nv && !core_sorted[s]) {
+        const int cnt = min(nn_sorted[s], list_cap);
+        int best = kNoCluster;
+        for (int q = 0; q < cnt; ++q) {
+            const int j = nbr_list[s * list_cap + q];
+            if (core_sorted[j]) best = min(best, cell_units ? cell_cid[pcell[j]] : ci_sorted[j]);
+        }
+        looked = (unsigned)cnt;
+        ci_sorted[s] = best;
+        ci_orig[perm[s]] = best;
+    }
+    looked = __reduce_add_sync(kFull, looked);
+    if ((threadIdx.x & 31) == 0 && looked) atomicAdd(pair_counter, (unsigned long long)looked);
 }
 
 // counters[1] += noise points; labels[rank[o]] = ci[o] for cores

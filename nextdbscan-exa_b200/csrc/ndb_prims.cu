@@ -131,19 +131,25 @@ __global__ void __launch_bounds__(kSortThreads) sort_upsweep_kernel(const K *__r
 // [w*256, w*256+256), item j of lane l is element w*256 + j*32 + l.  Ranks follow
 // that order (items in order, lanes in order within an item), warps follow each
 // other, and blocks follow each other through the digit-major histogram scan.
+// The tile is first reordered by digit in shared memory, so the global writes go
+// out as contiguous runs per digit instead of 32 scattered words per warp.
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
     const K *__restrict__ kin, const int32_t *__restrict__ vin, K *__restrict__ kout,
     int32_t *__restrict__ vout, int64_t n, int shift, const uint32_t *__restrict__ hist_scanned,
     int nblocks) {
     __shared__ uint32_t s_cnt[kSortWarps][kRadix];
-    __shared__ uint32_t s_base[kRadix];
+    __shared__ uint32_t s_base[kRadix];     // global position of the block's first element of each digit
+    __shared__ uint32_t s_local[kRadix];    // first tile position of each digit
+    __shared__ K s_key[kSortTile];
+    __shared__ int32_t s_val[kSortTile];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (int i = t; i < kSortWarps * kRadix; i += kSortThreads) (&s_cnt[0][0])[i] = 0;
     s_base[t] = hist_scanned[(int64_t)t * nblocks + blockIdx.x];
     __syncthreads();
 
-    const int64_t base = (int64_t)blockIdx.x * kSortTile + warp * (kSortItems * kWarp);
+    const int64_t tile0 = (int64_t)blockIdx.x * kSortTile;
+    const int64_t base = tile0 + warp * (kSortItems * kWarp);
     const unsigned lt = lanemask_lt();
     K key[kSortItems];
     int32_t val[kSortItems];
@@ -174,23 +180,52 @@ __global__ void __launch_bounds__(kSortThreads) sort_downsweep_kernel(
         __syncwarp();
     }
     __syncthreads();
-    {
-        uint32_t run = 0;
+    // per digit: exclusive prefix over warps, and the digit's total in the tile
+    uint32_t tot = 0;
 #pragma unroll
-        for (int w = 0; w < kSortWarps; ++w) {
-            const uint32_t c = s_cnt[w][t];
-            s_cnt[w][t] = run;
-            run += c;
+    for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = s_cnt[w][t];
+        s_cnt[w][t] = tot;
+        tot += c;
+    }
+    // exclusive scan of the digit totals over the 256 digits (one digit per thread)
+    {
+        uint32_t x = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
         }
+        __shared__ uint32_t s_w[kSortWarps];
+        if (lane == 31) s_w[warp] = x;
+        __syncthreads();
+        uint32_t wp = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w)
+            if (w < warp) wp += s_w[w];
+        s_local[t] = wp + x - tot;
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const int64_t e = base + j * kWarp + lane;
         if (e < n) {
-            const uint32_t pos = s_base[dig[j]] + s_cnt[warp][dig[j]] + rank[j];
-            kout[pos] = key[j];
-            vout[pos] = val[j];
+            const uint32_t lp = s_local[dig[j]] + s_cnt[warp][dig[j]] + rank[j];
+            s_key[lp] = key[j];
+            s_val[lp] = val[j];
+        }
+    }
+    __syncthreads();
+    const int valid_in_tile = (int)min((int64_t)kSortTile, n - tile0);
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i) {
+        const int e = i * kSortThreads + t;
+        if (e < valid_in_tile) {
+            const K k = s_key[e];
+            const uint32_t d = (uint32_t)(k >> shift) & 0xffu;
+            const uint32_t pos = s_base[d] + (uint32_t)e - s_local[d];
+            kout[pos] = k;
+            vout[pos] = s_val[e];
         }
     }
 }
