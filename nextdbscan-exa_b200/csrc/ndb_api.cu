@@ -24,7 +24,7 @@ struct ndb_ctx {
 
     // inputs / per-point arrays
     DevBuf coords, keys0, keys1, ids0, ids1, flags, pos, pcell, xs;
-    DevBuf nn_sorted, nn_orig, core_sorted, core_orig, rank, ci_sorted, ci_orig, labels;
+    DevBuf nn_sorted, nn_orig, core_sorted, core_bits, core_prefix, ci_sorted, ci_orig, labels;
     // per-cell arrays
     DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid, hash_keys, hash_vals;
     // union-find
@@ -51,6 +51,7 @@ struct ndb_ctx {
     int cell_units = 0;
     int n_rows = 0;
     unsigned long long hash_mask = 0;
+    int32_t *ci_user = nullptr;  // caller's cluster_index buffer of the current assign_labels call
     const float *coords_dev = nullptr;  // device coordinates of the current job
     GridDev grid{};
     Stencil stencil{};
@@ -368,17 +369,23 @@ void count_phase(ndb_ctx *ctx) {
 void core_flags_phase(ndb_ctx *ctx) {
     cudaStream_t st = ctx->stream;
     const int64_t n = ctx->n;
+    const int64_t n_words = (n + 31) / 32;
+    uint32_t *scal = small_at<uint32_t>(ctx, kSmallScalarOff);
     ensure(ctx, ctx->core_sorted, n + 1);
     ensure(ctx, ctx->cell_has_core, ctx->n_cells + 1);
-    ensure(ctx, ctx->nn_orig, (n + 1) * sizeof(int32_t));
-    ensure(ctx, ctx->core_orig, (n + 1) * sizeof(uint32_t));
-    ensure(ctx, ctx->rank, (n + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->core_bits, (n_words + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->core_prefix, (n_words + 1) * sizeof(uint32_t));
     ck(ctx, cudaMemsetAsync(ctx->cell_has_core.ptr, 0, ctx->n_cells + 1, st));
+    ck(ctx, cudaMemsetAsync(ctx->core_bits.ptr, 0, (n_words + 1) * sizeof(uint32_t), st));
     ++launch_counter(), core_flags_kernel<<<blocks_for(n), kBlock, 0, st>>>(
         ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->min_pts, ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(),
-        ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->nn_orig.as<int32_t>(),
-        ctx->core_orig.as<uint32_t>());
+        ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->core_bits.as<uint32_t>());
+    // ranks among cores in input order (data_process.cpp:276-283, :153): per-word prefix of the bitmap
+    ++launch_counter(), popc_words_kernel<<<blocks_for(n_words), kBlock, 0, st>>>(
+        ctx->core_bits.as<uint32_t>(), n_words, ctx->core_prefix.as<uint32_t>());
     ck(ctx, cudaGetLastError());
+    ck(ctx, scan_exclusive_u32(ctx->core_prefix.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), n_words, scal + 2,
+                               ctx->scan_scratch.as<uint32_t>(), st));
 }
 
 template <int D>
@@ -407,17 +414,11 @@ void labels_phase(ndb_ctx *ctx) {
     int *err = small_at<int>(ctx, kSmallErrOff);
     uint32_t *scal = small_at<uint32_t>(ctx, kSmallScalarOff);
 
-    // ranks among cores in input order (data_process.cpp:276-283, :153)
-    ck(ctx, scan_exclusive_u32(ctx->core_orig.as<uint32_t>(), ctx->rank.as<uint32_t>(), n, scal + 2,
-                               ctx->scan_scratch.as<uint32_t>(), st));
-
     const int64_t n_units = ctx->cell_units ? n_cells : nv;
     ensure(ctx, ctx->parent, (n_units + 1) * sizeof(int32_t));
     ensure(ctx, ctx->comp_min, (n_units + 1) * sizeof(int32_t));
     ensure(ctx, ctx->ci_sorted, (n + 1) * sizeof(int32_t));
-    ensure(ctx, ctx->ci_orig, (n + 1) * sizeof(int32_t));
     ensure(ctx, ctx->cell_cid, (n_cells + 1) * sizeof(int32_t));
-    ensure(ctx, ctx->labels, (n + 1) * sizeof(int32_t));
     ++launch_counter(), iota_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units);
     ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units, kNoCluster);
     ck(ctx, cudaGetLastError());
@@ -456,11 +457,11 @@ void labels_phase(ndb_ctx *ctx) {
     ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units, err);
     ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
         nv, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units,
-        ctx->rank.as<uint32_t>(), ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>());
-    ++launch_counter(), core_ids_kernel<<<blocks_for(n), kBlock, 0, st>>>(
-        nv, n, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units,
-        ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(), ctx->rank.as<uint32_t>(),
-        ctx->core_orig.as<uint32_t>(), ctx->ci_sorted.as<int32_t>(), ctx->ci_orig.as<int32_t>(), counters);
+        ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), ctx->parent.as<int32_t>(),
+        ctx->comp_min.as<int32_t>());
+    ++launch_counter(), core_ids_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+        nv, ctx->core_sorted.as<uint8_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units, ctx->parent.as<int32_t>(),
+        ctx->comp_min.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters);
     if (ctx->cell_units)
         ++launch_counter(), cell_ids_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(n_cells, ctx->cell_has_core.as<uint8_t>(),
                                                                 ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(),
@@ -472,19 +473,27 @@ void labels_phase(ndb_ctx *ctx) {
         ++launch_counter(), border_list_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
             nv, ctx->nn_sorted.as<int32_t>(), ctx->nbr_list.as<int32_t>(), ctx->list_cap,
             ctx->core_sorted.as<uint8_t>(), ctx->cell_units, ctx->pcell.as<int32_t>(), ctx->cell_cid.as<int32_t>(),
-            ctx->ids0.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), ctx->ci_orig.as<int32_t>(), counters + 4);
+            ctx->ci_sorted.as<int32_t>(), counters + 4);
         ck(ctx, cudaGetLastError());
     } else if (ctx->n_items > 0) {
         ++launch_counter(), border_kernel<D><<<grid, kBlock, 0, st>>>(
             ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
             ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-            ctx->cell_units, ctx->cell_cid.as<int32_t>(), ctx->ids0.as<int32_t>(), ctx->ci_sorted.as<int32_t>(),
-            ctx->ci_orig.as<int32_t>(), counters + 4);
+            ctx->cell_units, ctx->cell_cid.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters + 4);
         ck(ctx, cudaGetLastError());
     }
     cudaEventRecord(ctx->kev[7], st);
-    ++launch_counter(), meta_kernel<<<blocks_for(n), kBlock, 0, st>>>(n, ctx->ci_orig.as<int32_t>(), ctx->core_orig.as<uint32_t>(),
-                                                  ctx->rank.as<uint32_t>(), ctx->labels.as<int32_t>(), counters);
+    // ids in input order, straight into the caller's device buffer when there is one
+    int32_t *target = nullptr;
+    if (ctx->ci_user && (ctx->flags_run & NDB_FLAG_DEVICE_PTRS)) {
+        target = ctx->ci_user;
+    } else if (ctx->ci_user) {
+        ensure(ctx, ctx->ci_orig, (n + 1) * sizeof(int32_t));
+        target = ctx->ci_orig.as<int32_t>();
+    }
+    ++launch_counter(), output_ci_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+        ctx->ci_sorted.as<int32_t>(), nv, n, ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(),
+        ctx->core_prefix.as<uint32_t>(), target, counters);
     ck(ctx, cudaGetLastError());
     cudaEventRecord(ctx->ev[4], st);
 }
@@ -563,9 +572,16 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     classify_dispatch<D>(ctx, pl);
 
     if (nn_out) {
-        if (flags & NDB_FLAG_DEVICE_PTRS)
-            ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-        else
+        // counts in input order, straight into the caller's device buffer when there is one
+        int32_t *target = nn_out;
+        if (!(flags & NDB_FLAG_DEVICE_PTRS)) {
+            ensure(ctx, ctx->nn_orig, (n + 1) * sizeof(int32_t));
+            target = ctx->nn_orig.as<int32_t>();
+        }
+        ++launch_counter(), scatter_nn_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+            ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->ids0.as<int32_t>(), target);
+        ck(ctx, cudaGetLastError());
+        if (!(flags & NDB_FLAG_DEVICE_PTRS))
             ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     }
     unsigned long long h_counters[8];
@@ -591,14 +607,12 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
 template <int D>
 ndb_status labels_impl(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
     cudaStream_t st = ctx->stream;
+    ctx->ci_user = ci_out;
     labels_phase<D>(ctx);
+    ctx->ci_user = nullptr;
     const int64_t n = ctx->n;
-    if (ci_out) {
-        if (ctx->flags_run & NDB_FLAG_DEVICE_PTRS)
-            ck(ctx, cudaMemcpyAsync(ci_out, ctx->ci_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-        else
-            ck(ctx, cudaMemcpyAsync(ci_out, ctx->ci_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    }
+    if (ci_out && !(ctx->flags_run & NDB_FLAG_DEVICE_PTRS))
+        ck(ctx, cudaMemcpyAsync(ci_out, ctx->ci_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     unsigned long long h_counters[8];
     uint32_t h_scal[8];
     int h_err = 0;
@@ -710,7 +724,7 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);
     DevBuf *bufs[] = {&ctx->coords,      &ctx->keys0,     &ctx->keys1,      &ctx->ids0,        &ctx->ids1,
                       &ctx->flags,       &ctx->pos,       &ctx->pcell,      &ctx->xs,          &ctx->nn_sorted,
-                      &ctx->nn_orig,     &ctx->core_sorted, &ctx->core_orig, &ctx->rank,       &ctx->ci_sorted,
+                      &ctx->nn_orig,     &ctx->core_sorted, &ctx->core_bits, &ctx->core_prefix, &ctx->ci_sorted,
                       &ctx->ci_orig,     &ctx->labels,    &ctx->cell_start, &ctx->cell_key,    &ctx->nbr,
                       &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
                       &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small,
@@ -795,7 +809,12 @@ ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capa
     if (!ctx->have_labels) return NDB_ERR_NO_STATE;
     if (capacity < ctx->n_cores || (ctx->n_cores > 0 && !label_out)) return NDB_ERR_INVALID_ARGUMENT;
     if (ctx->n_cores == 0) return NDB_OK;
-    if (cudaMemcpyAsync(label_out, ctx->labels.ptr, ctx->n_cores * sizeof(int32_t), cudaMemcpyDeviceToHost,
+    if (ctx->labels.ensure((size_t)(ctx->n_cores + 1) * sizeof(int32_t)) != cudaSuccess) return NDB_ERR_OUT_OF_MEMORY;
+    ++launch_counter(), labels_kernel<<<blocks_for(ctx->n), kBlock, 0, ctx->stream>>>(
+        ctx->ci_sorted.as<int32_t>(), ctx->nv, ctx->n, ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(),
+        ctx->core_prefix.as<uint32_t>(), ctx->labels.as<int32_t>());
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(label_out, ctx->labels.ptr, ctx->n_cores * sizeof(int32_t), cudaMemcpyDeviceToHost,
                         ctx->stream) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return NDB_ERR_CUDA;
@@ -859,7 +878,7 @@ constexpr int kNaMaxRows = 25;  // largest stencil plan_grid builds (3-D, same-c
 // requests the pipeline makes: keys may be 64-bit, coordinates padded to 16).
 enum NaBuf {
     NA_KEYS0, NA_KEYS1, NA_IDS0, NA_IDS1, NA_FLAGS, NA_POS, NA_PCELL, NA_XS, NA_NN_SORTED, NA_NN_ORIG,
-    NA_CORE_SORTED, NA_CORE_ORIG, NA_RANK, NA_CI_SORTED, NA_CI_ORIG, NA_LABELS, NA_CELL_START, NA_CELL_KEY,
+    NA_CORE_SORTED, NA_CORE_BITS, NA_CORE_PREFIX, NA_CI_SORTED, NA_CI_ORIG, NA_LABELS, NA_CELL_START, NA_CELL_KEY,
     NA_NBR, NA_ITEM_CNT, NA_ITEMS, NA_CELL_HAS_CORE, NA_CELL_CID, NA_PARENT, NA_COMP_MIN, NA_SORT_HIST,
     NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_NBR_LIST, NA_COUNT
 };
@@ -897,7 +916,7 @@ NoAllocState g_na_state[kNaMaxDevices];
 DevBuf *na_buf(ndb_ctx &c, int b) {
     DevBuf *bufs[NA_COUNT] = {&c.keys0,       &c.keys1,     &c.ids0,      &c.ids1,         &c.flags,
                               &c.pos,         &c.pcell,     &c.xs,        &c.nn_sorted,    &c.nn_orig,
-                              &c.core_sorted, &c.core_orig, &c.rank,      &c.ci_sorted,    &c.ci_orig,
+                              &c.core_sorted, &c.core_bits, &c.core_prefix, &c.ci_sorted,  &c.ci_orig,
                               &c.labels,      &c.cell_start, &c.cell_key, &c.nbr,          &c.item_cnt,
                               &c.items,       &c.cell_has_core, &c.cell_cid, &c.parent,    &c.comp_min,
                               &c.sort_hist,   &c.scan_scratch, &c.small,     &c.hash_keys, &c.hash_vals,

@@ -45,7 +45,8 @@ struct Stencil {
 
 constexpr int kBlock = 256;
 constexpr int kMaxRowCells = 5;
-constexpr int kMaxListCap = 64;  // largest min_pts - 1 for which neighbour lists are kept  // cells per stencil row looked up together (2*xr+1 <= 5)
+constexpr int kMaxListCap = 64;  // largest min_pts - 1 for which neighbour lists are kept
+constexpr int kSmemListCap = 16;  // lists up to this length are staged in shared memory  // cells per stencil row looked up together (2*xr+1 <= 5)
 constexpr int kWarpsPerBlock = kBlock / kWarp;
 
 // ---------------------------------------------------------------------------
@@ -407,6 +408,8 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ RowTable s_rows[kWarpsPerBlock];
+    __shared__ int s_list[kWarpsPerBlock][kTile * kSmemListCap];
+    __shared__ int s_cnt[kWarpsPerBlock][kTile];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     if (item_id >= n_items) return;
@@ -414,6 +417,10 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     const int cell = item.x, p0 = item.y;
     const int cs = cell_start[cell], ce = cell_start[cell + 1];
     const int cnt = min(kTile, ce - p0);
+    // lists of up to kSmemListCap entries are gathered in shared memory and written
+    // out only for the points that end below min_pts; longer ones go straight out
+    const bool smem_list = list_cap <= kSmemListCap;
+    int *sl = s_list[wib];
     if (EARLY && dense_skip && ce - cs >= min_pts) {
         if (lane < cnt) nn_sorted[p0 + lane] = ce - cs;
         return;
@@ -426,9 +433,11 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         store_point_smem<D>(si + lane * P, x);
     }
     const int total = gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, rt, lane);
-    int c[kTile];
-#pragma unroll
-    for (int k = 0; k < kTile; ++k) c[k] = 0;
+    // running count of each of the item's points; every lane computes the same
+    // value and writes it, so the counter needs no per-lane copy
+    volatile int *cntk = s_cnt[wib];
+    cntk[lane] = 0;
+    __syncwarp();
     unsigned long long pairs = 0;
     for (int tb = 0; tb < total; tb += kWarp) {
         const int t = tb + lane;
@@ -437,59 +446,87 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         if (j >= 0) load_point<D>(xs, j, xj);
         else fill_nan<D>(xj);  // NaN fails the predicate
         int active = 0;
-#pragma unroll
-        for (int k = 0; k < kTile; ++k) {
+        for (int k = 0; k < cnt; ++k) {
+            const int ck = cntk[k];
             // a point that already reached min_pts (EARLY) needs no more tests
-            if (k < cnt && (!EARLY || c[k] < min_pts)) {
-                float xi[D];
-                load_point_smem<D>(si + k * P, xi);
-                const bool hit = in_range<D>(xi, xj, e2);
-                const unsigned m = __ballot_sync(kFull, hit);
-                // the first list_cap neighbours of each point; complete for every point
-                // whose count stays below min_pts (list_cap = min_pts - 1)
-                if (nbr_list && m && c[k] < list_cap) {
-                    const int slot = c[k] + __popc(m & lanemask_lt());
-                    if (hit && slot < list_cap) nbr_list[(int64_t)(p0 + k) * list_cap + slot] = j;
+            if (EARLY && ck >= min_pts) continue;
+            float xi[D];
+            load_point_smem<D>(si + k * P, xi);
+            const bool hit = in_range<D>(xi, xj, e2);
+            const unsigned m = __ballot_sync(kFull, hit);
+            // the first list_cap neighbours of each point; complete for every point
+            // whose count stays below min_pts (list_cap = min_pts - 1)
+            if (nbr_list && m && ck < list_cap) {
+                const int slot = ck + __popc(m & lanemask_lt());
+                if (hit && slot < list_cap) {
+                    if (smem_list) sl[k * kSmemListCap + slot] = j;
+                    else nbr_list[(int64_t)(p0 + k) * list_cap + slot] = j;
                 }
-                c[k] += __popc(m);
-                ++active;
             }
+            __syncwarp();
+            cntk[k] = ck + __popc(m);
+            ++active;
         }
+        __syncwarp();
         pairs += (unsigned long long)active * (unsigned long long)min(kWarp, total - tb);
-        if (EARLY) {
-            bool all = true;
-#pragma unroll
-            for (int k = 0; k < kTile; ++k) all = all && (k >= cnt || c[k] >= min_pts);
-            if (all) break;
+        if (EARLY && __all_sync(kFull, lane >= cnt || cntk[lane] >= min_pts)) break;
+    }
+    const int mine = lane < cnt ? cntk[lane] : 0;
+    if (lane < cnt) nn_sorted[p0 + lane] = mine;
+    if (nbr_list && smem_list) {
+        __syncwarp();
+        if (lane < cnt && mine < min_pts) {
+            const int len = min(mine, list_cap);
+            for (int q = 0; q < len; ++q) nbr_list[(int64_t)(p0 + lane) * list_cap + q] = sl[lane * kSmemListCap + q];
         }
     }
-    int mine = 0;
-#pragma unroll
-    for (int k = 0; k < kTile; ++k)
-        if (k == lane) mine = c[k];
-    if (lane < cnt) nn_sorted[p0 + lane] = mine;
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
 }
 
-// core flags in sorted and in input order; nn in input order
+// Core flags: per sorted point (u8), and a bitmap in input order (one bit per
+// point, atomicOr; 12.5 MB for 10^8 points, so it stays in L2).  With the
+// per-word prefix of its popcounts the bitmap gives every point's rank among the
+// cores in input order (data_process.cpp:276-283, :153) without a per-point scan.
 __global__ void core_flags_kernel(const int32_t *__restrict__ nn_sorted, int64_t nv, int64_t n, int min_pts,
                                   const int32_t *__restrict__ perm, const int32_t *__restrict__ pcell,
                                   uint8_t *__restrict__ core_sorted, uint8_t *__restrict__ cell_has_core,
-                                  int32_t *__restrict__ nn_orig, uint32_t *__restrict__ core_orig) {
+                                  uint32_t *__restrict__ core_bits) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const int32_t o = perm[s];
+    bool core;
     if (s < nv) {
-        const int32_t v = nn_sorted[s];
-        const bool core = v >= min_pts;
+        core = nn_sorted[s] >= min_pts;
         core_sorted[s] = core ? 1 : 0;
         if (core) cell_has_core[pcell[s]] = 1;
-        nn_orig[o] = v;
-        core_orig[o] = core ? 1u : 0u;
     } else {
-        nn_orig[o] = 0;
-        core_orig[o] = (0 >= min_pts) ? 1u : 0u;
+        core = 0 >= min_pts;  // points outside the grid have no neighbour, not even themselves
     }
+    if (core) {
+        const int32_t o = perm[s];
+        atomicOr(core_bits + (o >> 5), 1u << (o & 31));
+    }
+}
+
+__global__ void popc_words_kernel(const uint32_t *__restrict__ bits, int64_t n_words, uint32_t *__restrict__ cnt) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < n_words) cnt[w] = (uint32_t)__popc(bits[w]);
+}
+
+__device__ __forceinline__ bool is_core_o(const uint32_t *__restrict__ bits, int32_t o) {
+    return (bits[o >> 5] >> (o & 31)) & 1u;
+}
+
+// rank of point o among the cores, in input order
+__device__ __forceinline__ int32_t core_rank(const uint32_t *__restrict__ bits, const uint32_t *__restrict__ prefix,
+                                             int32_t o) {
+    return (int32_t)(prefix[o >> 5] + __popc(bits[o >> 5] & ((1u << (o & 31)) - 1u)));
+}
+
+// nn in input order (the caller's nn output)
+__global__ void scatter_nn_kernel(const int32_t *__restrict__ nn_sorted, int64_t nv, int64_t n,
+                                  const int32_t *__restrict__ perm, int32_t *__restrict__ out) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) out[perm[s]] = s < nv ? nn_sorted[s] : 0;
 }
 
 __global__ void iota_kernel(int32_t *__restrict__ a, int64_t n) {
@@ -810,14 +847,15 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
 // one lane per root issues the atomic (clusters have millions of cores).
 __global__ void comp_min_kernel(int64_t nv, const uint8_t *__restrict__ core_sorted,
                                 const int32_t *__restrict__ perm, const int32_t *__restrict__ pcell,
-                                int cell_units, const uint32_t *__restrict__ rank, const int32_t *__restrict__ parent,
+                                int cell_units, const uint32_t *__restrict__ core_bits,
+                                const uint32_t *__restrict__ core_prefix, const int32_t *__restrict__ parent,
                                 int32_t *__restrict__ comp_min) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool ok = s < nv && core_sorted[s];
     int root = -1, r = kNoCluster;
     if (ok) {
         root = parent[cell_units ? pcell[s] : (int)s];
-        r = (int)rank[perm[s]];
+        r = core_rank(core_bits, core_prefix, perm[s]);
     }
     unsigned pending = __ballot_sync(kFull, ok);
     const int lane = threadIdx.x & 31;
@@ -838,35 +876,21 @@ __global__ void flatten_kernel(int32_t *parent, int64_t n_units, int *err) {
     parent[u] = r;
 }
 
-// counters[0] = clusters (roots), counters[1] = noise
-__global__ void core_ids_kernel(int64_t nv, int64_t n, const uint8_t *__restrict__ core_sorted,
-                                const int32_t *__restrict__ perm, const int32_t *__restrict__ pcell,
-                                int cell_units, const int32_t *__restrict__ parent,
-                                const int32_t *__restrict__ comp_min, const uint32_t *__restrict__ rank,
-                                const uint32_t *__restrict__ core_orig, int32_t *__restrict__ ci_sorted,
-                                int32_t *__restrict__ ci_orig, unsigned long long *__restrict__ counters) {
+// ids of the cores in sorted order; counters[0] += component roots (point units)
+__global__ void core_ids_kernel(int64_t nv, const uint8_t *__restrict__ core_sorted,
+                                const int32_t *__restrict__ pcell, int cell_units,
+                                const int32_t *__restrict__ parent, const int32_t *__restrict__ comp_min,
+                                int32_t *__restrict__ ci_sorted, unsigned long long *__restrict__ counters) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned roots = 0;
     if (s < nv) {
         if (core_sorted[s]) {
             const int u = cell_units ? pcell[s] : (int)s;
             const int root = parent[u];
-            const int32_t cid = comp_min[root];
-            ci_sorted[s] = cid;
-            ci_orig[perm[s]] = cid;
+            ci_sorted[s] = comp_min[root];
             if (!cell_units && root == (int)s) roots = 1;
         } else {
             ci_sorted[s] = kNoCluster;
-        }
-    } else if (s < n) {
-        // points outside the grid: in range of nothing, so a core among them (only
-        // possible with min_pts <= 0) is a cluster of its own
-        const int32_t o = perm[s];
-        if (core_orig[o]) {
-            ci_orig[o] = (int32_t)rank[o];
-            roots = 1;
-        } else {
-            ci_orig[o] = kNoCluster;
         }
     }
     roots = __reduce_add_sync(kFull, roots);
@@ -907,8 +931,8 @@ __global__ void __launch_bounds__(kBlock) border_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2,
     const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core, int cell_units,
-    const int32_t *__restrict__ cell_cid, const int32_t *__restrict__ perm, int32_t *__restrict__ ci_sorted,
-    int32_t *__restrict__ ci_orig, unsigned long long *__restrict__ pair_counter) {
+    const int32_t *__restrict__ cell_cid, int32_t *__restrict__ ci_sorted,
+    unsigned long long *__restrict__ pair_counter) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ int s_idx[kWarpsPerBlock][kTile];
@@ -1036,11 +1060,7 @@ __global__ void __launch_bounds__(kBlock) border_kernel(
 #pragma unroll
     for (int k = 0; k < kTile; ++k)
         if (k == lane) mine_best = best[k];
-    if (lane < nb) {
-        const int s = sidx[lane];
-        ci_sorted[s] = mine_best;
-        ci_orig[perm[s]] = mine_best;
-    }
+    if (lane < nb) ci_sorted[sidx[lane]] = mine_best;
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
 }
 
@@ -1053,8 +1073,7 @@ __global__ void border_list_kernel(int64_t nv, const int32_t *__restrict__ nn_so
                                    const int32_t *__restrict__ nbr_list, int list_cap,
                                    const uint8_t *__restrict__ core_sorted, int cell_units,
                                    const int32_t *__restrict__ pcell, const int32_t *__restrict__ cell_cid,
-                                   const int32_t *__restrict__ perm, int32_t *__restrict__ ci_sorted,
-                                   int32_t *__restrict__ ci_orig, unsigned long long *__restrict__ pair_counter) {
+                                   int32_t *__restrict__ ci_sorted, unsigned long long *__restrict__ pair_counter) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned looked = 0;
     if (s < nv && !core_sorted[s]) {
@@ -1066,25 +1085,53 @@ __global__ void border_list_kernel(int64_t nv, const int32_t *__restrict__ nn_so
         }
         looked = (unsigned)cnt;
         ci_sorted[s] = best;
-        ci_orig[perm[s]] = best;
     }
     looked = __reduce_add_sync(kFull, looked);
     if ((threadIdx.x & 31) == 0 && looked) atomicAdd(pair_counter, (unsigned long long)looked);
 }
 
-// counters[1] += noise points; labels[rank[o]] = ci[o] for cores
-__global__ void meta_kernel(int64_t n, const int32_t *__restrict__ ci_orig, const uint32_t *__restrict__ core_orig,
-                            const uint32_t *__restrict__ rank, int32_t *__restrict__ labels,
-                            unsigned long long *__restrict__ counters) {
-    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned noise = 0;
-    if (o < n) {
-        const int32_t c = ci_orig[o];
-        if (c == kNoCluster) noise = 1;
-        if (core_orig[o]) labels[rank[o]] = c;
+// Cluster ids in input order (the caller's output; out may be null) and the
+// counts that need them: counters[1] += noise, counters[0] += cores outside the
+// grid (possible only with min_pts <= 0: in range of nothing, each is a cluster
+// of its own, numbered by its rank).
+__global__ void output_ci_kernel(const int32_t *__restrict__ ci_sorted, int64_t nv, int64_t n,
+                                 const int32_t *__restrict__ perm, const uint32_t *__restrict__ core_bits,
+                                 const uint32_t *__restrict__ core_prefix, int32_t *__restrict__ out,
+                                 unsigned long long *__restrict__ counters) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned noise = 0, roots = 0;
+    if (s < n) {
+        const int32_t o = perm[s];
+        int32_t v;
+        if (s < nv) {
+            v = ci_sorted[s];
+        } else if (is_core_o(core_bits, o)) {
+            v = core_rank(core_bits, core_prefix, o);
+            roots = 1;
+        } else {
+            v = kNoCluster;
+        }
+        noise = v == kNoCluster;
+        if (out) out[o] = v;
     }
     noise = __reduce_add_sync(kFull, noise);
-    if ((threadIdx.x & 31) == 0 && noise) atomicAdd(counters + 1, (unsigned long long)noise);
+    roots = __reduce_add_sync(kFull, roots);
+    if ((threadIdx.x & 31) == 0) {
+        if (noise) atomicAdd(counters + 1, (unsigned long long)noise);
+        if (roots) atomicAdd(counters + 0, (unsigned long long)roots);
+    }
+}
+
+// v_cluster_label in canonical form, on request: labels[rank(o)] = id of core o.
+__global__ void labels_kernel(const int32_t *__restrict__ ci_sorted, int64_t nv, int64_t n,
+                              const int32_t *__restrict__ perm, const uint32_t *__restrict__ core_bits,
+                              const uint32_t *__restrict__ core_prefix, int32_t *__restrict__ labels) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int32_t o = perm[s];
+    if (!is_core_o(core_bits, o)) return;
+    const int32_t r = core_rank(core_bits, core_prefix, o);
+    labels[r] = s < nv ? ci_sorted[s] : r;
 }
 
 }  // namespace ndb
