@@ -301,7 +301,7 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     // neighbour rows, through a hash table of the cells
     const int n_rows = pl.st.n_rows;
     int64_t hsize = 1024;
-    while (hsize < 2 * n_cells) hsize <<= 1;
+    while (hsize < 4 * n_cells) hsize <<= 1;  // load factor <= 1/4: most probes settle at the first slot
     ctx->hash_mask = (unsigned long long)(hsize - 1);
     ensure(ctx, ctx->hash_keys, hsize * sizeof(K));
     ensure(ctx, ctx->hash_vals, hsize * sizeof(int32_t));
@@ -312,7 +312,7 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
     int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
     ck(ctx, cudaMemcpyAsync(rows_dev, pl.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
-    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells * n_rows), kBlock, 0, st>>>(
+    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
         ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, ctx->hash_keys.as<K>(),
         ctx->hash_vals.as<int32_t>(), (unsigned long long)(hsize - 1), ctx->nbr.as<int2>());
     ck(ctx, cudaGetLastError());
@@ -894,8 +894,8 @@ constexpr size_t na_cap(int b) {
          : b == NA_SORT_HIST ? 4 * 256 * ((kNaN + kSortTile - 1) / kSortTile)
          : b == NA_SCAN ? 4 * 4096
          : b == NA_SMALL ? kSmallBytes
-         : b == NA_HASH_KEYS ? 8 * 2 * kNaN
-         : b == NA_HASH_VALS ? 4 * 2 * kNaN
+         : b == NA_HASH_KEYS ? 8 * 4 * kNaN
+         : b == NA_HASH_VALS ? 4 * 4 * kNaN
          : b == NA_NBR_LIST ? 4 * 16 * kNaN
          : 4 * (kNaN + 1);
 }

@@ -259,62 +259,70 @@ __device__ __forceinline__ int hash_find(const K *__restrict__ hkeys, const int3
 // nbr[c * n_rows + r] = [first, last) cell index of row r around cell c: the cells
 // of a row have consecutive keys, so the existing ones are consecutive in the
 // sorted cell list and the range runs from the smallest to the largest found.
+// Cell coordinates from a key (x fastest); 32-bit arithmetic for 32-bit keys.
+template <typename K>
+__device__ __forceinline__ void decode_key(K key, const GridDev &g, long long &x, long long &y, long long &z) {
+    if constexpr (sizeof(K) == 4) {
+        const uint32_t g0 = (uint32_t)g.g[0], g1 = (uint32_t)g.g[1];
+        const uint32_t rest = (uint32_t)key / g0;
+        x = (long long)((uint32_t)key - rest * g0);
+        y = g.k >= 3 ? (long long)(rest % g1) : (long long)rest;
+        z = g.k >= 3 ? (long long)(rest / g1) : 0;
+    } else {
+        const unsigned long long g0 = (unsigned long long)g.g[0], g1 = (unsigned long long)g.g[1];
+        const unsigned long long rest = (unsigned long long)key / g0;
+        x = (long long)((unsigned long long)key - rest * g0);
+        y = g.k >= 3 ? (long long)(rest % g1) : (long long)rest;
+        z = g.k >= 3 ? (long long)(rest / g1) : 0;
+    }
+}
+
+// nbr[c * n_rows + r] = [first, last) cell index of row r around cell c: the cells
+// of a row have consecutive keys, so the existing ones are consecutive in the
+// sorted cell list and the range runs from the smallest to the largest found.
+// One thread per cell (one key decode); the first hash probes of a row's cells
+// are issued together.
 template <typename K>
 __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell_key, int64_t n_cells,
                                                       GridDev g, const int4 *__restrict__ rows, int n_rows,
                                                       const K *__restrict__ hkeys, const int32_t *__restrict__ hvals,
                                                       unsigned long long mask, int2 *__restrict__ nbr) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n_cells * n_rows) return;
-    const int64_t c = idx / n_rows;
-    const int r = (int)(idx - c * n_rows);
-    const unsigned long long key = (unsigned long long)cell_key[c];
-    const unsigned long long g0 = (unsigned long long)g.g[0], g1 = (unsigned long long)g.g[1];
-    const long long c0 = (long long)(key % g0);
-    const unsigned long long rest = key / g0;
-    const long long c1 = g.k >= 3 ? (long long)(rest % g1) : (long long)rest;
-    const long long c2 = g.k >= 3 ? (long long)(rest / g1) : 0;
-    const int4 row = __ldg(rows + r);
-    const long long y = c1 + row.x, z = c2 + row.y;
-    int2 out = make_int2(0, 0);
-    const bool in = (g.k < 2 || (y >= 0 && y < g.g[1])) && (g.k < 3 || (z >= 0 && z < g.g[2]));
-    if (in) {
-        const long long x0 = c0 - row.z < 0 ? 0 : c0 - row.z;
-        const long long x1 = c0 + row.z > g.g[0] - 1 ? g.g[0] - 1 : c0 + row.z;
-        unsigned long long base = 0;
-        if (g.k >= 2) base += (unsigned long long)y * g.stride[1];
-        if (g.k >= 3) base += (unsigned long long)z * g.stride[2];
-        int lo = 0x7fffffff, hi = -1;
-        // first probes of all (at most kMaxRowCells) cells of the row issued together
-        unsigned long long slot[kMaxRowCells];
-        K seen[kMaxRowCells];
-#pragma unroll
-        for (int q = 0; q < kMaxRowCells; ++q) {
-            slot[q] = hash_slot(base + (unsigned long long)(x0 + q), mask);
-            seen[q] = (x0 + q <= x1) ? __ldg(hkeys + slot[q]) : ~(K)0;
-        }
-#pragma unroll
-        for (int q = 0; q < kMaxRowCells; ++q) {
-            if (x0 + q > x1) continue;
-            const unsigned long long want = base + (unsigned long long)(x0 + q);
-            int ci = -1;
-            if ((unsigned long long)seen[q] == want) ci = __ldg(hvals + slot[q]);
-            else if (seen[q] != ~(K)0) ci = hash_find(hkeys, hvals, mask, want);
-            if (ci >= 0) {
-                lo = min(lo, ci);
-                hi = max(hi, ci);
+    __shared__ int4 s_rows[kMaxRows];
+    for (int r = threadIdx.x; r < n_rows; r += blockDim.x) s_rows[r] = rows[r];
+    __syncthreads();
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    long long cx, cy, cz;
+    decode_key<K>(cell_key[c], g, cx, cy, cz);
+    int2 *out = nbr + c * n_rows;
+    for (int r = 0; r < n_rows; ++r) {
+        const int4 row = s_rows[r];
+        const long long y = cy + row.x, z = cz + row.y;
+        int2 res = make_int2(0, 0);
+        const bool in = (g.k < 2 || (y >= 0 && y < g.g[1])) && (g.k < 3 || (z >= 0 && z < g.g[2]));
+        if (in) {
+            const long long x0 = cx - row.z < 0 ? 0 : cx - row.z;
+            const long long x1 = cx + row.z > g.g[0] - 1 ? g.g[0] - 1 : cx + row.z;
+            unsigned long long base = 0;
+            if (g.k >= 2) base += (unsigned long long)y * g.stride[1];
+            if (g.k >= 3) base += (unsigned long long)z * g.stride[2];
+            // the row's existing cells are consecutive in the sorted cell list: find the
+            // first one by hashing (usually the first probe, at x0), then walk the keys
+            int ca = -1;
+            for (long long xx = x0; xx <= x1 && ca < 0; ++xx)
+                ca = hash_find(hkeys, hvals, mask, base + (unsigned long long)xx);
+            int lo = 0x7fffffff, hi = -1;
+            if (ca >= 0) {
+                const unsigned long long kmax = base + (unsigned long long)x1;
+                int cb = ca + 1;
+                while (cb < n_cells && (unsigned long long)__ldg(cell_key + cb) <= kmax) ++cb;
+                lo = ca;
+                hi = cb - 1;
             }
+            if (hi >= 0) res = make_int2(lo, hi + 1);
         }
-        for (long long xx = x0 + kMaxRowCells; xx <= x1; ++xx) {
-            const int ci = hash_find(hkeys, hvals, mask, base + (unsigned long long)xx);
-            if (ci >= 0) {
-                lo = min(lo, ci);
-                hi = max(hi, ci);
-            }
-        }
-        if (hi >= 0) out = make_int2(lo, hi + 1);
+        out[r] = res;
     }
-    nbr[idx] = out;
 }
 
 __global__ void item_count_kernel(const int32_t *__restrict__ cell_start, int64_t n_cells,
@@ -631,11 +639,8 @@ __global__ void __launch_bounds__(kBlock) union_near_kernel(
     if (idx < n_cells && cell_has_core[idx]) {
         const int A = (int)idx;
         const unsigned long long key = (unsigned long long)cell_key[A];
-        const unsigned long long g0 = (unsigned long long)g.g[0], g1 = (unsigned long long)g.g[1];
-        const unsigned long long rest = key / g0;
-        const long long x = (long long)(key - rest * g0);
-        const long long y = g.k >= 3 ? (long long)(rest % g1) : (long long)rest;
-        const long long z = g.k >= 3 ? (long long)(rest / g1) : 0;
+        long long x, y, z;
+        decode_key<K>(cell_key[A], g, x, y, z);
         int nb[3] = {-1, -1, -1};
         if (x + 1 < g.g[0] && A + 1 < n_cells && (unsigned long long)cell_key[A + 1] == key + 1ull) nb[0] = A + 1;
         if (g.k >= 2 && y + 1 < g.g[1]) nb[1] = hash_find(hkeys, hvals, mask, key + g.stride[1]);
