@@ -86,7 +86,7 @@ typedef struct ndb_stats {
     int64_t n_valid;          /* points that took part in the grid */
     int64_t n_cells;          /* non-empty grid cells */
     int64_t n_tiles;          /* work items (cell chunks of up to 32 points) */
-    int32_t grid_dims;        /* gridded dimensions (1..3) */
+    int32_t grid_dims;        /* gridded dimensions (1..4) */
     int32_t stencil_rows;     /* neighbour rows per cell */
     int32_t same_cell_linked; /* 1 when all points of a cell are provably within eps */
     int32_t key_bits;         /* radix-sort key width actually sorted */

@@ -106,7 +106,7 @@ T *small_at(ndb_ctx *ctx, size_t off) {
 // w * (1 + 2^-20) per dimension, so their FP32 length is below
 // d * w^2 * (1 + 2^-19) * (1 + 2^-24)^5 < e2: every pair inside a cell is in range.
 // Otherwise (or when a dimension would need more than the per-dimension cell cap)
-// up to three dimensions are gridded with cells of at least r * (1 + 2^-12).
+// up to four dimensions are gridded with cells of at least r * (1 + 2^-12).
 //
 // Stencil: cell coordinates of an accepted pair differ by at most
 // R = ceil(r / w + 2^-18) per dimension (the 2^-18 covers the cell-coordinate
@@ -128,11 +128,12 @@ Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
     r *= 1.0 + ldexp(1.0, -20);
     const double slack = ldexp(1.0, -18);
 
-    auto cap_for = [](int k) { return k >= 3 ? ldexp(1.0, 20) : ldexp(1.0, 30); };
+    // cells per gridded dimension: keys stay below 2^62 and cell coordinates exact in double
+    auto cap_for = [](int k) { return k >= 4 ? ldexp(1.0, 15) : k == 3 ? ldexp(1.0, 20) : ldexp(1.0, 30); };
 
     int k = 0;
-    int dims[3] = {0, 0, 0};
-    double w[3] = {1, 1, 1};
+    int dims[kMaxGridDims] = {0, 0, 0, 0};
+    double w[kMaxGridDims] = {1, 1, 1, 1};
     bool linked = false;
     if (d <= 3 && (double)e2 >= ldexp(1.0, -100)) {
         const double wl = sqrt((double)e2 / d * (1.0 - ldexp(1.0, -10)));
@@ -148,10 +149,10 @@ Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
         }
     }
     if (!linked) {
-        k = d < 3 ? d : 3;
+        // up to four dimensions, the widest ones (input order kept among them)
+        k = d < kMaxGridDims ? d : kMaxGridDims;
         std::vector<int> order(d);
         for (int a = 0; a < d; ++a) order[a] = a;
-        // grid the k widest dimensions, keeping input order among them
         std::stable_sort(order.begin(), order.end(),
                          [&](int x, int y) { return (hi[x] - lo[x]) > (hi[y] - lo[y]); });
         std::sort(order.begin(), order.begin() + k);
@@ -166,7 +167,7 @@ Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
     pl.g.k = k;
     unsigned long long stride = 1;
     double total = 1;
-    for (int a = 0; a < 3; ++a) {
+    for (int a = 0; a < kMaxGridDims; ++a) {
         if (a < k) {
             const double span = hi[dims[a]] - lo[dims[a]];
             pl.g.dim[a] = dims[a];
@@ -189,10 +190,10 @@ Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
     while (bits < 64 && ldexp(1.0, bits) - 1.0 < total) ++bits;
     pl.key_bits = bits;
 
-    int R[3] = {0, 0, 0};
+    int R[kMaxGridDims] = {0, 0, 0, 0};
     for (int a = 0; a < k; ++a) R[a] = (int)ceil(r / w[a] + slack);
     struct Row {
-        int o1, o2, xr;
+        int o1, o2, o3, xr;
         double dist2;
     };
     std::vector<Row> rows;
@@ -201,26 +202,29 @@ Plan plan_grid(int d, float e2, const double *lo, const double *hi) {
         return q > 0 ? q * w[a] : 0.0;
     };
     const double r2 = r * r;
-    for (int o2 = -R[2]; o2 <= R[2]; ++o2) {
-        for (int o1 = -R[1]; o1 <= R[1]; ++o1) {
-            const double g1 = k >= 2 ? gap(o1, 1) : 0.0, g2 = k >= 3 ? gap(o2, 2) : 0.0;
-            const double base = g1 * g1 + g2 * g2;
-            if (base > r2) continue;
-            int xr = 0;
-            for (int o0 = 1; o0 <= R[0]; ++o0) {
-                const double g0 = gap(o0, 0);
-                if (base + g0 * g0 <= r2) xr = o0;
+    for (int o3 = -R[3]; o3 <= R[3]; ++o3) {
+        for (int o2 = -R[2]; o2 <= R[2]; ++o2) {
+            for (int o1 = -R[1]; o1 <= R[1]; ++o1) {
+                const double g1 = k >= 2 ? gap(o1, 1) : 0.0, g2 = k >= 3 ? gap(o2, 2) : 0.0,
+                             g3 = k >= 4 ? gap(o3, 3) : 0.0;
+                const double base = g1 * g1 + g2 * g2 + g3 * g3;
+                if (base > r2) continue;
+                int xr = 0;
+                for (int o0 = 1; o0 <= R[0]; ++o0) {
+                    const double g0 = gap(o0, 0);
+                    if (base + g0 * g0 <= r2) xr = o0;
+                }
+                rows.push_back({o1, o2, o3, xr, base});
             }
-            rows.push_back({o1, o2, xr, base});
         }
     }
     std::stable_sort(rows.begin(), rows.end(), [](const Row &x, const Row &y) {
         if (x.dist2 != y.dist2) return x.dist2 < y.dist2;
-        return std::abs(x.o1) + std::abs(x.o2) < std::abs(y.o1) + std::abs(y.o2);
+        return std::abs(x.o1) + std::abs(x.o2) + std::abs(x.o3) < std::abs(y.o1) + std::abs(y.o2) + std::abs(y.o3);
     });
     pl.st.n_rows = (int)rows.size();
     for (size_t i = 0; i < rows.size() && i < (size_t)kMaxRows; ++i)
-        pl.st.rows[i] = make_int4(rows[i].o1, rows[i].o2, rows[i].xr, 0);
+        pl.st.rows[i] = make_int4(rows[i].o1, rows[i].o2, rows[i].o3, rows[i].xr);
     return pl;
 }
 
@@ -872,7 +876,7 @@ namespace {
 
 constexpr size_t na_align(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kNaN = NDB_NOALLOC_MAX_POINTS;
-constexpr int kNaMaxRows = 25;  // largest stencil plan_grid builds (3-D, same-cell-linked cells)
+constexpr int kNaMaxRows = 27;  // largest stencil plan_grid builds (4 gridded dimensions: 3^3 rows)
 
 // Capacity of each buffer for jobs of up to kNaN points (upper bounds of the
 // requests the pipeline makes: keys may be 64-bit, coordinates padded to 16).

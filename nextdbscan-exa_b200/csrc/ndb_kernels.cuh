@@ -21,26 +21,30 @@
 
 #include <float.h>
 
+#include <type_traits>
+
 #include "ndb_common.cuh"
 
 namespace ndb {
 
 // Grid description passed by value to the kernels.
+constexpr int kMaxGridDims = 4;
+
 struct GridDev {
-    int k;                   // gridded dimensions (1..3)
-    int dim[3];              // input dimension of each gridded dimension
-    double lo[3];            // origin per gridded dimension
-    double inv_w[3];         // 1 / cell width
-    long long g[3];          // cells per gridded dimension
-    unsigned long long stride[3];  // key strides (1, g0, g0*g1)
+    int k;                                  // gridded dimensions (1..4)
+    int dim[kMaxGridDims];                  // input dimension of each gridded dimension
+    double lo[kMaxGridDims];                // origin per gridded dimension
+    double inv_w[kMaxGridDims];             // 1 / cell width
+    long long g[kMaxGridDims];              // cells per gridded dimension
+    unsigned long long stride[kMaxGridDims];  // key strides (1, g0, g0*g1, g0*g1*g2)
 };
 
 // Neighbour rows of a cell.  Row r covers the cells at offsets (x in
-// [-xr, +xr], o1, o2) in gridded dimensions (0, 1, 2); those cells have
+// [-xr, +xr], o1, o2, o3) in gridded dimensions (0, 1, 2, 3); those cells have
 // consecutive keys, hence form one contiguous run of the sorted cell list.
 struct Stencil {
     int n_rows;
-    int4 rows[kMaxRows];  // (o1, o2, xr, unused), nearest rows first
+    int4 rows[kMaxRows];  // (o1, o2, o3, xr), nearest rows first
 };
 
 constexpr int kBlock = 256;
@@ -153,7 +157,7 @@ __global__ void __launch_bounds__(kBlock) key_kernel(const float *__restrict__ c
     if (point_valid<D>(p)) {
         unsigned long long kk = 0;
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < kMaxGridDims; ++a)
             if (a < g.k) kk += (unsigned long long)cell_coord(g, a, p[g.dim[a]]) * g.stride[a];
         key = (K)kk;
     }
@@ -261,6 +265,29 @@ __device__ __forceinline__ int hash_find(const K *__restrict__ hkeys, const int3
 // sorted cell list and the range runs from the smallest to the largest found.
 // Cell coordinates from a key (x fastest); 32-bit arithmetic for 32-bit keys.
 template <typename K>
+__device__ __forceinline__ void decode_key(K key, const GridDev &g, long long (&c)[kMaxGridDims]) {
+    using U = typename std::conditional<sizeof(K) == 4, uint32_t, unsigned long long>::type;
+    U rest = (U)key;
+#pragma unroll
+    for (int a = 0; a < kMaxGridDims; ++a) {
+        if (a < g.k - 1) {
+            const U ga = (U)g.g[a];
+            const U q = rest / ga;
+            c[a] = (long long)(rest - q * ga);
+            rest = q;
+        } else if (a == g.k - 1) {
+            c[a] = (long long)rest;
+        } else {
+            c[a] = 0;
+        }
+    }
+}
+
+// nbr[c * n_rows + r] = [first, last) cell index of row r around cell c: the cells
+// of a row have consecutive keys, so the existing ones are consecutive in the
+// sorted cell list and the range runs from the smallest to the largest found.
+// Cell coordinates from a key (x fastest); 32-bit arithmetic for 32-bit keys.
+template <typename K>
 __device__ __forceinline__ void decode_key(K key, const GridDev &g, long long &x, long long &y, long long &z) {
     if constexpr (sizeof(K) == 4) {
         const uint32_t g0 = (uint32_t)g.g[0], g1 = (uint32_t)g.g[1];
@@ -292,20 +319,26 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
     __syncthreads();
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n_cells) return;
-    long long cx, cy, cz;
-    decode_key<K>(cell_key[c], g, cx, cy, cz);
+    long long cc[kMaxGridDims];
+    decode_key<K>(cell_key[c], g, cc);
     int2 *out = nbr + c * n_rows;
     for (int r = 0; r < n_rows; ++r) {
         const int4 row = s_rows[r];
-        const long long y = cy + row.x, z = cz + row.y;
+        const int off[kMaxGridDims] = {0, row.x, row.y, row.z};
+        bool in = true;
+        unsigned long long base = 0;
+#pragma unroll
+        for (int a = 1; a < kMaxGridDims; ++a) {
+            if (a < g.k) {
+                const long long v = cc[a] + off[a];
+                in = in && v >= 0 && v < g.g[a];
+                base += (unsigned long long)(v < 0 ? 0 : v) * g.stride[a];
+            }
+        }
         int2 res = make_int2(0, 0);
-        const bool in = (g.k < 2 || (y >= 0 && y < g.g[1])) && (g.k < 3 || (z >= 0 && z < g.g[2]));
         if (in) {
-            const long long x0 = cx - row.z < 0 ? 0 : cx - row.z;
-            const long long x1 = cx + row.z > g.g[0] - 1 ? g.g[0] - 1 : cx + row.z;
-            unsigned long long base = 0;
-            if (g.k >= 2) base += (unsigned long long)y * g.stride[1];
-            if (g.k >= 3) base += (unsigned long long)z * g.stride[2];
+            const long long x0 = cc[0] - row.w < 0 ? 0 : cc[0] - row.w;
+            const long long x1 = cc[0] + row.w > g.g[0] - 1 ? g.g[0] - 1 : cc[0] + row.w;
             // the row's existing cells are consecutive in the sorted cell list: find the
             // first one by hashing (usually the first probe, at x0), then walk the keys
             int ca = -1;
@@ -639,12 +672,12 @@ __global__ void __launch_bounds__(kBlock) union_near_kernel(
     if (idx < n_cells && cell_has_core[idx]) {
         const int A = (int)idx;
         const unsigned long long key = (unsigned long long)cell_key[A];
-        long long x, y, z;
-        decode_key<K>(cell_key[A], g, x, y, z);
+        long long cc[kMaxGridDims];
+        decode_key<K>(cell_key[A], g, cc);
         int nb[3] = {-1, -1, -1};
-        if (x + 1 < g.g[0] && A + 1 < n_cells && (unsigned long long)cell_key[A + 1] == key + 1ull) nb[0] = A + 1;
-        if (g.k >= 2 && y + 1 < g.g[1]) nb[1] = hash_find(hkeys, hvals, mask, key + g.stride[1]);
-        if (g.k >= 3 && z + 1 < g.g[2]) nb[2] = hash_find(hkeys, hvals, mask, key + g.stride[2]);
+        if (cc[0] + 1 < g.g[0] && A + 1 < n_cells && (unsigned long long)cell_key[A + 1] == key + 1ull) nb[0] = A + 1;
+        if (g.k >= 2 && cc[1] + 1 < g.g[1]) nb[1] = hash_find(hkeys, hvals, mask, key + g.stride[1]);
+        if (g.k >= 3 && cc[2] + 1 < g.g[2]) nb[2] = hash_find(hkeys, hvals, mask, key + g.stride[2]);
         bool any = false;
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
