@@ -476,10 +476,12 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     const int total = gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, rt, lane);
     // running count of each of the item's points; every lane computes the same
     // value and writes it, so the counter needs no per-lane copy
-    volatile int *cntk = s_cnt[wib];
+    int *cntk = s_cnt[wib];
     cntk[lane] = 0;
     __syncwarp();
     unsigned long long pairs = 0;
+    // points still counting (EARLY: below min_pts); warp-uniform
+    unsigned act = __ballot_sync(kFull, lane < cnt);
     for (int tb = 0; tb < total; tb += kWarp) {
         const int t = tb + lane;
         const int j = t < total ? row_lookup(rt, n_rows, t) : -1;
@@ -487,10 +489,9 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         if (j >= 0) load_point<D>(xs, j, xj);
         else fill_nan<D>(xj);  // NaN fails the predicate
         int active = 0;
-        for (int k = 0; k < cnt; ++k) {
+        for (unsigned it = act; it; it &= it - 1) {
+            const int k = __ffs(it) - 1;
             const int ck = cntk[k];
-            // a point that already reached min_pts (EARLY) needs no more tests
-            if (EARLY && ck >= min_pts) continue;
             float xi[D];
             load_point_smem<D>(si + k * P, xi);
             const bool hit = in_range<D>(xi, xj, e2);
@@ -510,7 +511,10 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         }
         __syncwarp();
         pairs += (unsigned long long)active * (unsigned long long)min(kWarp, total - tb);
-        if (EARLY && __all_sync(kFull, lane >= cnt || cntk[lane] >= min_pts)) break;
+        if (EARLY) {
+            act = __ballot_sync(kFull, lane < cnt && cntk[lane] < min_pts);
+            if (!act) break;
+        }
     }
     const int mine = lane < cnt ? cntk[lane] : 0;
     if (lane < cnt) nn_sorted[p0 + lane] = mine;
@@ -846,21 +850,26 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     for (int tb = 0; tb < total; tb += kWarp) {
         // roots of the item's cores, refreshed every chunk so that candidates already
         // joined to them are skipped before the predicate
-        if (lane < nc) sroot[lane] = uf_find(parent, sidx[lane], err);
+        int myroot = lane < nc ? uf_find(parent, sidx[lane], err) : -1;
+        if (lane < nc) sroot[lane] = myroot;
+        // one root for all of the item's cores (the usual case once they are joined)
+        const int root0 = __shfl_sync(kFull, myroot, 0);
+        const bool uniform = __all_sync(kFull, lane >= nc || myroot == root0);
         __syncwarp();
         const int t = tb + lane;
         int j = -1;
         if (t < total) j = row_lookup(rt, n_rows, t);
-        const bool valid = j > p0 && core_sorted[j];
+        bool valid = j > p0 && core_sorted[j];
         float xj[D];
         int pj = -1;
         if (valid) {
-            load_point<D>(xs, j, xj);
             pj = __ldcg(parent + j);
             pj = __ldcg(parent + pj);  // two hops: an ancestor of j, usually its root
-        } else {
-            fill_nan<D>(xj);
+            if (uniform && pj == root0) valid = false;  // joined to every core of the item already
         }
+        if (!__any_sync(kFull, valid)) continue;
+        if (valid) load_point<D>(xs, j, xj);
+        else fill_nan<D>(xj);
         int tested = 0;
         for (int k = 0; k < nc; ++k) {
             const int ik = sidx[k];
