@@ -138,6 +138,29 @@ ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d,
                         int32_t min_pts, uint32_t flags, int32_t *nn_out,
                         int32_t *cluster_index_out, ndb_result *result);
 
+/* One job of a batched run: an independent DBSCAN problem with its own
+ * coordinates, dimensionality, eps and min_pts (the arguments of one
+ * ndb_b200_run call).  result and status are written by ndb_b200_run_batched. */
+typedef struct ndb_job {
+    const float *coords;        /* n x d FP32, row-major; device memory with NDB_FLAG_DEVICE_PTRS */
+    int64_t n;
+    int32_t d;
+    float eps;
+    int32_t min_pts;
+    int32_t *nn_out;            /* n int32 or NULL */
+    int32_t *cluster_index_out; /* n int32 or NULL */
+    ndb_result result;          /* out */
+    int32_t status;             /* out: ndb_status of this job */
+} ndb_job;
+
+/* Runs many independent jobs as one pipeline: jobs of the same dimensionality
+ * are concatenated, every phase is one launch over all of them (per-job eps,
+ * min_pts and grid are looked up per cell), and results land in each job's own
+ * buffers.  Results are identical to one ndb_b200_run per job.  No counterpart
+ * in the reference, which clusters one input per process (nextdbscan.cpp:28-68).
+ * Returns the first failing job's status (each job also carries its own). */
+ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t n_jobs, uint32_t flags);
+
 /* Per-core label array of the last run, the reference's v_cluster_label
  * (data_process.h:58, filled at data_process.cpp:141-260): entry k is the cluster id
  * of the k-th core point, so label[k] == k exactly for the reference's roots

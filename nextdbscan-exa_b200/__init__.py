@@ -150,6 +150,37 @@ class Context:
         self.n = n
         return Result(res.clusters, res.noise, res.core_count, res.n)
 
+    # -- many independent problems in one pipeline ----------------------------
+    def run_batched(self, problems, *, full_count: bool = False, approximate: bool = False,
+                    want_nn: bool = True) -> list[tuple[np.ndarray | None, np.ndarray, Result]]:
+        """problems: iterable of (coords n x d, eps, min_pts).  Returns per problem
+        (nn, cluster_index, Result), equal to one run() each.  Raises NdbError on
+        the first failing problem's status after every other one has run."""
+        problems = list(problems)
+        pts = [_as_points(c) for c, _, _ in problems]
+        jobs = (lib.NdbJob * len(pts))()
+        outs = []
+        for j, ((_, eps, m), x) in enumerate(zip(problems, pts)):
+            nn = np.empty(x.shape[0], dtype=np.int32) if want_nn else None
+            ci = np.empty(x.shape[0], dtype=np.int32)
+            jobs[j].coords = x.ctypes.data if x.size else None
+            jobs[j].n, jobs[j].d = x.shape
+            jobs[j].eps, jobs[j].min_pts = float(eps), int(m)
+            jobs[j].nn_out = nn.ctypes.data if nn is not None and nn.size else None
+            jobs[j].cluster_index_out = ci.ctypes.data if ci.size else None
+            outs.append((nn, ci))
+        flags = (lib.FLAG_FULL_COUNT if full_count else 0) | (lib.FLAG_APPROXIMATE if approximate else 0)
+        st = self._lib.ndb_b200_run_batched(self._h, jobs, len(pts), flags)
+        self.last_jobs = jobs
+        lib.check(st, "ndb_b200_run_batched", self._h)
+        return [(nn, ci, Result(jobs[j].result.clusters, jobs[j].result.noise, jobs[j].result.core_count,
+                                jobs[j].result.n)) for j, (nn, ci) in enumerate(outs)]
+
+    def run_batched_jobs(self, jobs, n_jobs: int, flags: int) -> int:
+        """Raw form: jobs is a ctypes array of lib.NdbJob (addresses filled by the
+        caller, host or device per flags).  Returns the status without raising."""
+        return self._lib.ndb_b200_run_batched(self._h, jobs, int(n_jobs), int(flags))
+
     def cluster_label(self, core_count: int) -> np.ndarray:
         out = np.empty(max(core_count, 0), dtype=np.int32)
         st = self._lib.ndb_b200_cluster_label(self._h, out.ctypes.data if core_count > 0 else None, core_count)

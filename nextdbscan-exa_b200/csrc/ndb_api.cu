@@ -1,6 +1,8 @@
 // ndb_api.cu -- context, grid planning and the extern "C" entry points of
 // libndb_b200.so (declared in include/ndb_b200.h).
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -35,6 +37,8 @@ struct ndb_ctx {
     int list_cap = 0;                 // entries per point, 0 when the lists are off
     // scratch
     DevBuf sort_hist, scan_scratch, small;  // small: counters, bbox, scalars
+    // batched runs: job table, per-job bounding boxes, cell -> job, per-job counters
+    DevBuf jobs_dev, batch_bbox, cell_job, job_counters;
 
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     // kernel-level events: sort, count, union, border (begin, end)
@@ -318,7 +322,7 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     ck(ctx, cudaMemcpyAsync(rows_dev, pl.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
     ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
         ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, ctx->hash_keys.as<K>(),
-        ctx->hash_vals.as<int32_t>(), (unsigned long long)(hsize - 1), ctx->nbr.as<int2>());
+        ctx->hash_vals.as<int32_t>(), (unsigned long long)(hsize - 1), ctx->nbr.as<int2>(), nullptr, nullptr);
     ck(ctx, cudaGetLastError());
 
     // work items
@@ -359,12 +363,12 @@ void count_phase(ndb_ctx *ctx) {
             ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                 ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
-                ctx->list_cap, counters + 2);
+                ctx->list_cap, ctx->list_cap, counters + 2, nullptr, nullptr);
         else
             ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                 ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
-                ctx->list_cap, counters + 2);
+                ctx->list_cap, ctx->list_cap, counters + 2, nullptr, nullptr);
         ck(ctx, cudaGetLastError());
     }
     cudaEventRecord(ctx->kev[3], st);
@@ -383,7 +387,8 @@ void core_flags_phase(ndb_ctx *ctx) {
     ck(ctx, cudaMemsetAsync(ctx->core_bits.ptr, 0, (n_words + 1) * sizeof(uint32_t), st));
     ++launch_counter(), core_flags_kernel<<<blocks_for(n), kBlock, 0, st>>>(
         ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->min_pts, ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(),
-        ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->core_bits.as<uint32_t>());
+        ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->core_bits.as<uint32_t>(), nullptr,
+        nullptr, 0);
     // ranks among cores in input order (data_process.cpp:276-283, :153): per-word prefix of the bitmap
     ++launch_counter(), popc_words_kernel<<<blocks_for(n_words), kBlock, 0, st>>>(
         ctx->core_bits.as<uint32_t>(), n_words, ctx->core_prefix.as<uint32_t>());
@@ -436,25 +441,25 @@ void labels_phase(ndb_ctx *ctx) {
                     n_cells, ctx->grid, ctx->cell_key.as<uint64_t>(), ctx->cell_start.as<int32_t>(),
                     ctx->hash_keys.as<uint64_t>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask, ctx->xs.as<float>(),
                     ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                    ctx->parent.as<int32_t>(), counters + 3, err);
+                    ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
             else
                 ++launch_counter(), union_near_kernel<D, uint32_t><<<blocks_for(n_cells), kBlock, 0, st>>>(
                     n_cells, ctx->grid, ctx->cell_key.as<uint32_t>(), ctx->cell_start.as<int32_t>(),
                     ctx->hash_keys.as<uint32_t>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask, ctx->xs.as<float>(),
                     ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                    ctx->parent.as<int32_t>(), counters + 3, err);
+                    ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
             ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                       n_units, err);
             ++launch_counter(), union_cells_kernel<D><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
                 n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->xs.as<float>(),
                 ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
-                counters + 3, err);
+                counters + 3, err, nullptr, nullptr);
         }
         else
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                 ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                ctx->parent.as<int32_t>(), counters + 3, err);
+                ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
         ck(ctx, cudaGetLastError());
     }
     cudaEventRecord(ctx->kev[5], st);
@@ -465,11 +470,11 @@ void labels_phase(ndb_ctx *ctx) {
         ctx->comp_min.as<int32_t>());
     ++launch_counter(), core_ids_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
         nv, ctx->core_sorted.as<uint8_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units, ctx->parent.as<int32_t>(),
-        ctx->comp_min.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters);
+        ctx->comp_min.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters, nullptr, nullptr);
     if (ctx->cell_units)
         ++launch_counter(), cell_ids_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(n_cells, ctx->cell_has_core.as<uint8_t>(),
                                                                 ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(),
-                                                                ctx->cell_cid.as<int32_t>(), counters);
+                                                                ctx->cell_cid.as<int32_t>(), counters, nullptr, nullptr);
     ck(ctx, cudaGetLastError());
     cudaEventRecord(ctx->ev[3], st);
     cudaEventRecord(ctx->kev[6], st);
@@ -497,7 +502,7 @@ void labels_phase(ndb_ctx *ctx) {
     }
     ++launch_counter(), output_ci_kernel<<<blocks_for(n), kBlock, 0, st>>>(
         ctx->ci_sorted.as<int32_t>(), nv, n, ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(),
-        ctx->core_prefix.as<uint32_t>(), target, counters);
+        ctx->core_prefix.as<uint32_t>(), target, counters, nullptr, 0, nullptr);
     ck(ctx, cudaGetLastError());
     cudaEventRecord(ctx->ev[4], st);
 }
@@ -583,7 +588,7 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
             target = ctx->nn_orig.as<int32_t>();
         }
         ++launch_counter(), scatter_nn_kernel<<<blocks_for(n), kBlock, 0, st>>>(
-            ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->ids0.as<int32_t>(), target);
+            ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->ids0.as<int32_t>(), target, nullptr, 0);
         ck(ctx, cudaGetLastError());
         if (!(flags & NDB_FLAG_DEVICE_PTRS))
             ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -732,7 +737,8 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
                       &ctx->ci_orig,     &ctx->labels,    &ctx->cell_start, &ctx->cell_key,    &ctx->nbr,
                       &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
                       &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small,
-                      &ctx->hash_keys,   &ctx->hash_vals, &ctx->nbr_list};
+                      &ctx->hash_keys,   &ctx->hash_vals, &ctx->nbr_list, &ctx->jobs_dev,
+                      &ctx->batch_bbox,  &ctx->cell_job,  &ctx->job_counters};
     for (DevBuf *b : bufs) b->release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -853,6 +859,474 @@ const char *ndb_b200_last_cuda_error(ndb_ctx *ctx) { return ctx ? ctx->last_cuda
 const char *ndb_b200_version(void) { return NDB_VERSION; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched runs (ndb_b200_run_batched)
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kMaxBatchPoints = int64_t(1) << 30;  // points of one pipeline (int32 indices, headroom)
+
+struct BatchPlan {
+    std::vector<JobDev> jd;  // per member, in member order
+    Stencil st{};
+    int key_bits = 0;
+    int linked = 0;
+    int list_stride = 0;
+    int64_t total_n = 0, nv = 0;
+};
+
+template <int D, typename K>
+void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, BatchPlan &bp, uint32_t flags) {
+    cudaStream_t st = ctx->stream;
+    constexpr int P = Stride<D>::P;
+    const int nj = (int)members.size();
+    const int64_t n = bp.total_n, nv = bp.nv;
+    const JobDev *jobs_dev = ctx->jobs_dev.as<JobDev>();
+    unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
+    int *err = small_at<int>(ctx, kSmallErrOff);
+    uint32_t *scal = small_at<uint32_t>(ctx, kSmallScalarOff);
+    int64_t max_n = 1;
+    for (auto &j : bp.jd) max_n = std::max<int64_t>(max_n, j.n);
+    const unsigned gx = (unsigned)std::min<int64_t>((max_n + kBlock - 1) / kBlock, 64);
+
+    // composite keys and the sort
+    ensure(ctx, ctx->keys0, n * sizeof(K));
+    ensure(ctx, ctx->keys1, n * sizeof(K));
+    ensure(ctx, ctx->ids0, n * sizeof(int32_t));
+    ensure(ctx, ctx->ids1, n * sizeof(int32_t));
+    ensure(ctx, ctx->sort_hist, sort_hist_words(n) * sizeof(uint32_t));
+    const size_t scan_words = std::max(scan_scratch_words(n + 1), scan_scratch_words((int64_t)sort_hist_words(n)));
+    ensure(ctx, ctx->scan_scratch, (scan_words + 64) * sizeof(uint32_t));
+    const K invalid_key = (K)(bp.key_bits >= (int)(8 * sizeof(K)) ? ~(K)0 : (((K)1 << bp.key_bits) - 1));
+    ++launch_counter(), key_batch_kernel<D, K><<<dim3(gx, nj), kBlock, 0, st>>>(
+        ctx->coords.as<float>(), jobs_dev, invalid_key, ctx->keys0.as<K>(), ctx->ids0.as<int32_t>());
+    ck(ctx, cudaGetLastError());
+    bool in_first = true;
+    if (sizeof(K) == 4)
+        ck(ctx, radix_sort_pairs_u32(reinterpret_cast<uint32_t *>(ctx->keys0.ptr), ctx->ids0.as<int32_t>(),
+                                     reinterpret_cast<uint32_t *>(ctx->keys1.ptr), ctx->ids1.as<int32_t>(), n,
+                                     bp.key_bits, ctx->sort_hist.as<uint32_t>(), ctx->scan_scratch.as<uint32_t>(),
+                                     &in_first, st));
+    else
+        ck(ctx, radix_sort_pairs_u64(reinterpret_cast<uint64_t *>(ctx->keys0.ptr), ctx->ids0.as<int32_t>(),
+                                     reinterpret_cast<uint64_t *>(ctx->keys1.ptr), ctx->ids1.as<int32_t>(), n,
+                                     bp.key_bits, ctx->sort_hist.as<uint32_t>(), ctx->scan_scratch.as<uint32_t>(),
+                                     &in_first, st));
+    if (!in_first) {
+        std::swap(ctx->keys0, ctx->keys1);
+        std::swap(ctx->ids0, ctx->ids1);
+    }
+    const K *keys = ctx->keys0.as<K>();
+    const int32_t *perm = ctx->ids0.as<int32_t>();
+
+    // cells
+    ensure(ctx, ctx->flags, (n + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->pos, (n + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->pcell, (n + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->cell_start, (n + 2) * sizeof(int32_t));
+    ensure(ctx, ctx->cell_key, (n + 1) * sizeof(K));
+    ++launch_counter(), cell_flag_kernel<K><<<blocks_for(nv), kBlock, 0, st>>>(keys, nv, ctx->flags.as<uint32_t>());
+    ck(ctx, scan_exclusive_u32(ctx->flags.as<uint32_t>(), ctx->pos.as<uint32_t>(), nv, scal + 0,
+                               ctx->scan_scratch.as<uint32_t>(), st));
+    ++launch_counter(), cell_write_kernel<K><<<blocks_for(nv), kBlock, 0, st>>>(
+        keys, nv, ctx->pos.as<uint32_t>(), scal + 0, ctx->cell_start.as<int32_t>(), ctx->cell_key.as<K>(),
+        ctx->pcell.as<int32_t>());
+    ensure(ctx, ctx->xs, (nv + 1) * P * sizeof(float));
+    ++launch_counter(), gather_kernel<D><<<blocks_for(nv), kBlock, 0, st>>>(ctx->coords.as<float>(), perm, nv,
+                                                                           ctx->xs.as<float>());
+    ck(ctx, cudaGetLastError());
+    uint32_t n_cells32 = 0;
+    ck(ctx, cudaMemcpyAsync(&n_cells32, scal + 0, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+    const int64_t n_cells = nv > 0 ? n_cells32 : 0;
+    ensure(ctx, ctx->cell_job, (n_cells + 1) * sizeof(int32_t));
+    ++launch_counter(), cell_job_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, jobs_dev, nj, ctx->cell_job.as<int32_t>());
+    const int32_t *cell_job = ctx->cell_job.as<int32_t>();
+
+    // neighbour rows through the cell hash table
+    const int n_rows = bp.st.n_rows;
+    int64_t hsize = 1024;
+    while (hsize < 4 * n_cells) hsize <<= 1;
+    const unsigned long long hmask = (unsigned long long)(hsize - 1);
+    ensure(ctx, ctx->hash_keys, hsize * sizeof(K));
+    ensure(ctx, ctx->hash_vals, hsize * sizeof(int32_t));
+    ++launch_counter(), hash_clear_kernel<K><<<blocks_for(hsize), kBlock, 0, st>>>(ctx->hash_keys.as<K>(), hsize);
+    ++launch_counter(), hash_insert_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, ctx->hash_keys.as<K>(), ctx->hash_vals.as<int32_t>(), hmask);
+    ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
+    int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
+    ck(ctx, cudaMemcpyAsync(rows_dev, bp.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
+    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, bp.jd[0].g, rows_dev, n_rows, ctx->hash_keys.as<K>(),
+        ctx->hash_vals.as<int32_t>(), hmask, ctx->nbr.as<int2>(), jobs_dev, cell_job);
+    ck(ctx, cudaGetLastError());
+
+    // work items
+    ensure(ctx, ctx->item_cnt, (n_cells + 1) * sizeof(uint32_t));
+    ++launch_counter(), item_count_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
+        ctx->cell_start.as<int32_t>(), n_cells, ctx->item_cnt.as<uint32_t>());
+    ck(ctx, scan_exclusive_u32(ctx->item_cnt.as<uint32_t>(), ctx->item_cnt.as<uint32_t>(), n_cells, scal + 1,
+                               ctx->scan_scratch.as<uint32_t>(), st));
+    uint32_t n_items32 = 0;
+    ck(ctx, cudaMemcpyAsync(&n_items32, scal + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+    const int64_t n_items = n_cells > 0 ? n_items32 : 0;
+    ensure(ctx, ctx->items, (n_items + 1) * sizeof(int2));
+    ++launch_counter(), item_write_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
+        ctx->cell_start.as<int32_t>(), n_cells, ctx->item_cnt.as<uint32_t>(), ctx->items.as<int2>());
+
+    // neighbour counts and core flags
+    ensure(ctx, ctx->nn_sorted, (n + 1) * sizeof(int32_t));
+    int32_t *list = nullptr;
+    if (bp.list_stride > 0) {
+        ensure(ctx, ctx->nbr_list, (size_t)(nv * bp.list_stride + 1) * sizeof(int32_t));
+        list = ctx->nbr_list.as<int32_t>();
+    }
+    const unsigned grid = (unsigned)((n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    const bool early = (flags & NDB_FLAG_FULL_COUNT) == 0;
+    if (n_items > 0) {
+        if (early)
+            ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
+                ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
+                ctx->xs.as<float>(), 0.0f, 0, 0, ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, counters + 2,
+                jobs_dev, cell_job);
+        else
+            ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
+                ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
+                ctx->xs.as<float>(), 0.0f, 0, 0, ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, counters + 2,
+                jobs_dev, cell_job);
+        ck(ctx, cudaGetLastError());
+    }
+    const int64_t n_words = (n + 31) / 32;
+    ensure(ctx, ctx->core_sorted, n + 1);
+    ensure(ctx, ctx->cell_has_core, n_cells + 1);
+    ensure(ctx, ctx->core_bits, (n_words + 1) * sizeof(uint32_t));
+    ensure(ctx, ctx->core_prefix, (n_words + 1) * sizeof(uint32_t));
+    ck(ctx, cudaMemsetAsync(ctx->cell_has_core.ptr, 0, n_cells + 1, st));
+    ck(ctx, cudaMemsetAsync(ctx->core_bits.ptr, 0, (n_words + 1) * sizeof(uint32_t), st));
+    ++launch_counter(), core_flags_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+        ctx->nn_sorted.as<int32_t>(), nv, n, 0, perm, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(),
+        ctx->cell_has_core.as<uint8_t>(), ctx->core_bits.as<uint32_t>(), jobs_dev, cell_job, nj);
+    ++launch_counter(), popc_words_kernel<<<blocks_for(n_words), kBlock, 0, st>>>(
+        ctx->core_bits.as<uint32_t>(), n_words, ctx->core_prefix.as<uint32_t>());
+    ck(ctx, cudaGetLastError());
+    ck(ctx, scan_exclusive_u32(ctx->core_prefix.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), n_words, scal + 2,
+                               ctx->scan_scratch.as<uint32_t>(), st));
+
+    // union-find, canonical ids, border points
+    const int64_t n_units = bp.linked ? n_cells : nv;
+    ensure(ctx, ctx->parent, (n_units + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->comp_min, (n_units + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->ci_sorted, (n + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->cell_cid, (n_cells + 1) * sizeof(int32_t));
+    ensure(ctx, ctx->job_counters, (size_t)(4 * nj + 4) * sizeof(unsigned long long));
+    unsigned long long *jc = ctx->job_counters.as<unsigned long long>();
+    ck(ctx, cudaMemsetAsync(jc, 0, (size_t)(4 * nj + 4) * sizeof(unsigned long long), st));
+    ++launch_counter(), iota_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units);
+    ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units,
+                                                                           kNoCluster);
+    if (n_items > 0) {
+        if (bp.linked) {
+            ++launch_counter(), union_near_kernel<D, K><<<blocks_for(n_cells), kBlock, 0, st>>>(
+                n_cells, bp.jd[0].g, ctx->cell_key.as<K>(), ctx->cell_start.as<int32_t>(), ctx->hash_keys.as<K>(),
+                ctx->hash_vals.as<int32_t>(), hmask, ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(),
+                ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err, jobs_dev, cell_job);
+            ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
+                                                                                      n_units, err);
+            ++launch_counter(), union_cells_kernel<D><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
+                n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows, ctx->xs.as<float>(), 0.0f,
+                ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
+                counters + 3, err, jobs_dev, cell_job);
+        } else {
+            ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
+                ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
+                ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+                ctx->parent.as<int32_t>(), counters + 3, err, jobs_dev, cell_job);
+        }
+        ck(ctx, cudaGetLastError());
+    }
+    ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units, err);
+    ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+        nv, ctx->core_sorted.as<uint8_t>(), perm, ctx->pcell.as<int32_t>(), bp.linked, ctx->core_bits.as<uint32_t>(),
+        ctx->core_prefix.as<uint32_t>(), ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>());
+    ++launch_counter(), core_ids_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+        nv, ctx->core_sorted.as<uint8_t>(), ctx->pcell.as<int32_t>(), bp.linked, ctx->parent.as<int32_t>(),
+        ctx->comp_min.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters, cell_job, jc);
+    if (bp.linked)
+        ++launch_counter(), cell_ids_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
+            n_cells, ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(),
+            ctx->cell_cid.as<int32_t>(), counters, cell_job, jc);
+    if (bp.list_stride > 0)
+        ++launch_counter(), border_list_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+            nv, ctx->nn_sorted.as<int32_t>(), list, bp.list_stride, ctx->core_sorted.as<uint8_t>(), bp.linked,
+            ctx->pcell.as<int32_t>(), ctx->cell_cid.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters + 4);
+    ck(ctx, cudaGetLastError());
+
+    // outputs straight into each job's buffers, per-job meta
+    ++launch_counter(), scatter_nn_kernel<<<blocks_for(n), kBlock, 0, st>>>(ctx->nn_sorted.as<int32_t>(), nv, n, perm,
+                                                                           nullptr, jobs_dev, nj);
+    ++launch_counter(), output_ci_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+        ctx->ci_sorted.as<int32_t>(), nv, n, perm, ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(),
+        nullptr, counters, jobs_dev, nj, jc);
+    ++launch_counter(), job_cores_kernel<<<blocks_for(nj), kBlock, 0, st>>>(
+        jobs_dev, nj, ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), n, jc);
+    ck(ctx, cudaGetLastError());
+    std::vector<unsigned long long> h_jc((size_t)4 * nj);
+    int h_err = 0;
+    ck(ctx, cudaMemcpyAsync(h_jc.data(), jc, (size_t)4 * nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st));
+    ck(ctx, cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (!(flags & NDB_FLAG_DEVICE_PTRS)) {
+        for (int m = 0; m < nj; ++m) {
+            ndb_job &J = jobs[members[m]];
+            const int64_t off = bp.jd[m].off;
+            if (J.nn_out)
+                ck(ctx, cudaMemcpyAsync(J.nn_out, ctx->nn_orig.as<int32_t>() + off, J.n * sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, st));
+            if (J.cluster_index_out)
+                ck(ctx, cudaMemcpyAsync(J.cluster_index_out, ctx->ci_orig.as<int32_t>() + off, J.n * sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, st));
+        }
+    }
+    ck(ctx, cudaStreamSynchronize(st));
+    for (int m = 0; m < nj; ++m) {
+        ndb_job &J = jobs[members[m]];
+        J.result.clusters = (int32_t)h_jc[4 * m + 0];
+        J.result.noise = (int32_t)h_jc[4 * m + 1];
+        J.result.core_count = (int32_t)h_jc[4 * m + 2];
+        J.result.n = (int32_t)J.n;
+        J.status = h_err ? NDB_ERR_DEVICE_LIMIT : NDB_OK;
+    }
+}
+
+// One pipeline over jobs of dimensionality D (members: indices into jobs).  Jobs
+// the pipeline cannot take (a grid of another kind, min_pts beyond the neighbour-
+// list cap, key space exhausted) are moved to `solo` and the pipeline is rebuilt
+// over the rest, so it only ever holds jobs it runs.
+template <int D>
+void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uint32_t flags,
+               std::vector<int> &solo) {
+    if (members.empty()) return;
+    cudaStream_t st = ctx->stream;
+    const int nj = (int)members.size();
+    BatchPlan bp;
+    bp.jd.resize(nj);
+    int64_t off = 0, max_n = 1;
+    for (int m = 0; m < nj; ++m) {
+        const ndb_job &J = jobs[members[m]];
+        JobDev &jd = bp.jd[m];
+        memset(&jd, 0, sizeof(jd));
+        jd.off = off;
+        jd.n = J.n;
+        jd.e2 = J.eps * J.eps;  // data_process.h:73
+        jd.min_pts = J.min_pts;
+        jd.src = J.coords;
+        off += J.n;
+        max_n = std::max<int64_t>(max_n, J.n);
+    }
+    bp.total_n = off;
+    const int64_t n = off;
+    ensure(ctx, ctx->coords, (size_t)n * D * sizeof(float));
+    ensure(ctx, ctx->jobs_dev, (size_t)nj * sizeof(JobDev));
+    ck(ctx, cudaMemcpyAsync(ctx->jobs_dev.ptr, bp.jd.data(), (size_t)nj * sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    const unsigned gx = (unsigned)std::min<int64_t>((max_n + kBlock - 1) / kBlock, 64);
+    if (flags & NDB_FLAG_DEVICE_PTRS) {
+        ++launch_counter(), gather_jobs_kernel<D><<<dim3(gx, nj), kBlock, 0, st>>>(ctx->jobs_dev.as<JobDev>(),
+                                                                                  ctx->coords.as<float>());
+        ck(ctx, cudaGetLastError());
+    } else {
+        for (int m = 0; m < nj; ++m)
+            if (jobs[members[m]].n > 0)
+                ck(ctx, cudaMemcpyAsync(ctx->coords.as<float>() + bp.jd[m].off * D, jobs[members[m]].coords,
+                                        (size_t)jobs[members[m]].n * D * sizeof(float), cudaMemcpyHostToDevice, st));
+    }
+
+    // per-job bounding boxes, then every job's grid planned on the host (one sync)
+    const size_t lh_bytes = ((size_t)nj * 2 * D * sizeof(int) + 15) & ~size_t(15);
+    ensure(ctx, ctx->batch_bbox, lh_bytes + (size_t)nj * sizeof(unsigned long long) + 64);
+    int *lo_hi = ctx->batch_bbox.as<int>();
+    unsigned long long *inval = reinterpret_cast<unsigned long long *>(ctx->batch_bbox.as<char>() + lh_bytes);
+    ++launch_counter(), bbox_batch_init_kernel<<<blocks_for((int64_t)nj * D), kBlock, 0, st>>>(lo_hi, D, nj, inval);
+    ++launch_counter(), bbox_batch_kernel<D><<<dim3(gx, nj), kBlock, 0, st>>>(ctx->coords.as<float>(),
+                                                                             ctx->jobs_dev.as<JobDev>(), lo_hi, inval);
+    ck(ctx, cudaGetLastError());
+    std::vector<int> h_lo_hi((size_t)nj * 2 * D);
+    std::vector<unsigned long long> h_inval(nj);
+    ck(ctx, cudaMemcpyAsync(h_lo_hi.data(), lo_hi, h_lo_hi.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaMemcpyAsync(h_inval.data(), inval, nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaStreamSynchronize(st));
+
+    auto dec = [](int v) {
+        const int i = v >= 0 ? v : v ^ 0x7fffffff;
+        float f;
+        memcpy(&f, &i, sizeof(f));
+        return (double)f;
+    };
+    unsigned long long key_base = 0;
+    bool have_stencil = false;
+    bp.linked = D <= 3 ? 1 : 0;
+    int64_t nv = 0;
+    std::vector<int> kept;
+    for (int m = 0; m < nj; ++m) {
+        JobDev &jd = bp.jd[m];
+        const int64_t jnv = jd.n - (int64_t)h_inval[m];
+        double lo[kMaxDim], hi[kMaxDim];
+        for (int a = 0; a < D; ++a) {
+            lo[a] = jnv > 0 ? dec(h_lo_hi[(size_t)m * 2 * D + a]) : 0.0;
+            hi[a] = jnv > 0 ? dec(h_lo_hi[(size_t)m * 2 * D + D + a]) : 0.0;
+        }
+        const Plan pl = plan_grid(D, jd.e2, lo, hi);
+        double cells = 1;
+        for (int a = 0; a < pl.g.k; ++a) cells *= (double)pl.g.g[a];
+        bool keep = (pl.cell_units ? 1 : 0) == bp.linked && jd.min_pts - 1 <= kMaxListCap &&
+                    (double)key_base + cells < ldexp(1.0, 62);
+        if (keep && have_stencil) keep = pl.st.n_rows == bp.st.n_rows;
+        if (!keep) {
+            solo.push_back(members[m]);
+            continue;
+        }
+        kept.push_back(members[m]);
+        if (!have_stencil) {
+            bp.st = pl.st;
+            have_stencil = true;
+        }
+        jd.g = pl.g;
+        jd.linked = bp.linked;
+        jd.list_cap = std::max(0, jd.min_pts - 1);
+        jd.key_base = key_base;  // every job owns >= 1 key, so the bases increase
+        key_base += (unsigned long long)cells;
+        bp.list_stride = std::max(bp.list_stride, jd.list_cap);
+        nv += jnv;
+    }
+    if ((int)kept.size() != nj) {
+        run_group<D>(ctx, jobs, kept, flags, solo);  // the pipeline over the jobs it can run
+        return;
+    }
+    bp.nv = nv;
+    // the all-ones key of invalid points must exceed every composite key
+    int bits = 1;
+    while (bits < 64 && ldexp(1.0, bits) - 1.0 < (double)key_base) ++bits;
+    bp.key_bits = bits;
+    if (getenv("NDB_DEBUG")) {
+        for (int m = 0; m < nj; ++m)
+            fprintf(stderr, "ndb batch d=%d job %d: off=%lld n=%lld invalid=%llu key_base=%llu k=%d\n", D, members[m],
+                    (long long)bp.jd[m].off, (long long)bp.jd[m].n, h_inval[m], bp.jd[m].key_base, bp.jd[m].g.k);
+    }
+    // outputs: device pointers go straight to the kernels; host ones through staging
+    if (flags & NDB_FLAG_DEVICE_PTRS) {
+        for (int m = 0; m < nj; ++m) {
+            bp.jd[m].nn_out = jobs[members[m]].nn_out;
+            bp.jd[m].ci_out = jobs[members[m]].cluster_index_out;
+        }
+    } else {
+        ensure(ctx, ctx->nn_orig, (n + 1) * sizeof(int32_t));
+        ensure(ctx, ctx->ci_orig, (n + 1) * sizeof(int32_t));
+        for (int m = 0; m < nj; ++m) {
+            bp.jd[m].nn_out = jobs[members[m]].nn_out ? ctx->nn_orig.as<int32_t>() + bp.jd[m].off : nullptr;
+            bp.jd[m].ci_out = jobs[members[m]].cluster_index_out ? ctx->ci_orig.as<int32_t>() + bp.jd[m].off : nullptr;
+        }
+    }
+    ck(ctx, cudaMemcpyAsync(ctx->jobs_dev.ptr, bp.jd.data(), (size_t)nj * sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    if (bits <= 32) run_group_keys<D, uint32_t>(ctx, jobs, members, bp, flags);
+    else run_group_keys<D, uint64_t>(ctx, jobs, members, bp, flags);
+}
+
+template <int D>
+ndb_status run_group_entry(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uint32_t flags,
+                           std::vector<int> &solo) {
+    try {
+        run_group<D>(ctx, jobs, members, flags, solo);
+        return NDB_OK;
+    } catch (const Fail &f) {
+        for (int m : members)
+            if (jobs[m].status == NDB_OK) jobs[m].status = f.st;
+        return f.st;
+    }
+}
+
+}  // namespace
+
+extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t n_jobs, uint32_t flags) {
+    ndb_status s = check_ctx(ctx);
+    if (s != NDB_OK) return s;
+    if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return NDB_ERR_INVALID_ARGUMENT;
+    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS)) return NDB_ERR_INVALID_ARGUMENT;
+    ctx->have_state = false;
+    ctx->have_labels = false;
+    ctx->stats = ndb_stats{};
+    launch_counter() = 0;
+    if (ctx->small.ensure(kSmallBytes) != cudaSuccess) return NDB_ERR_OUT_OF_MEMORY;
+    if (cudaMemsetAsync(ctx->small.ptr, 0, kSmallBytes, ctx->stream) != cudaSuccess) return NDB_ERR_CUDA;
+    ndb_status first = NDB_OK;
+    // validate, and group by dimensionality
+    std::vector<std::vector<int>> groups(NDB_MAX_DIM + 1);
+    for (int64_t i = 0; i < n_jobs; ++i) {
+        ndb_job &J = jobs[i];
+        J.result = ndb_result{0, 0, 0, (int32_t)(J.n > 0 ? J.n : 0)};
+        J.status = NDB_OK;
+        const float e2 = J.eps * J.eps;
+        if (J.d < 1 || J.d > NDB_MAX_DIM) J.status = NDB_ERR_UNSUPPORTED_DIM;
+        else if (J.n < 0 || (J.n > 0 && !J.coords)) J.status = NDB_ERR_INVALID_ARGUMENT;
+        else if (J.n > NDB_MAX_POINTS) J.status = NDB_ERR_TOO_MANY_POINTS;
+        else if (!isfinite(e2)) J.status = NDB_ERR_INVALID_EPS;
+        if (J.status != NDB_OK) {
+            if (first == NDB_OK) first = (ndb_status)J.status;
+            continue;
+        }
+        if (J.n == 0) continue;
+        groups[J.d].push_back((int)i);
+    }
+    std::vector<int> solo;
+    for (int d = 1; d <= NDB_MAX_DIM; ++d) {
+        // pipelines of at most kMaxBatchPoints points
+        size_t b = 0;
+        while (b < groups[d].size()) {
+            std::vector<int> members;
+            int64_t pts = 0;
+            while (b < groups[d].size() && (members.empty() || pts + jobs[groups[d][b]].n <= kMaxBatchPoints)) {
+                pts += jobs[groups[d][b]].n;
+                members.push_back(groups[d][b++]);
+            }
+#define NDB_GROUP(D) run_group_entry<D>(ctx, jobs, members, flags, solo)
+            ndb_status gs;
+            switch (d) {
+                case 1: gs = NDB_GROUP(1); break;
+                case 2: gs = NDB_GROUP(2); break;
+                case 3: gs = NDB_GROUP(3); break;
+                case 4: gs = NDB_GROUP(4); break;
+                case 5: gs = NDB_GROUP(5); break;
+                case 6: gs = NDB_GROUP(6); break;
+                case 7: gs = NDB_GROUP(7); break;
+                case 8: gs = NDB_GROUP(8); break;
+                case 9: gs = NDB_GROUP(9); break;
+                case 10: gs = NDB_GROUP(10); break;
+                case 11: gs = NDB_GROUP(11); break;
+                case 12: gs = NDB_GROUP(12); break;
+                case 13: gs = NDB_GROUP(13); break;
+                case 14: gs = NDB_GROUP(14); break;
+                case 15: gs = NDB_GROUP(15); break;
+                default: gs = NDB_GROUP(16); break;
+            }
+#undef NDB_GROUP
+            if (gs != NDB_OK && first == NDB_OK) first = gs;
+        }
+    }
+    // jobs the pipeline could not take: one call each
+    for (int i : solo) {
+        ndb_job &J = jobs[i];
+        ndb_result r{};
+        const ndb_status js = ndb_b200_run(ctx, J.coords, J.n, J.d, J.eps, J.min_pts, flags, J.nn_out,
+                                           J.cluster_index_out, &r);
+        J.status = js;
+        if (js == NDB_OK) J.result = r;
+        else if (first == NDB_OK) first = js;
+    }
+    ctx->have_state = false;
+    ctx->have_labels = false;
+    return first;
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free entry point (ndb_b200_run_noalloc).

@@ -47,6 +47,34 @@ struct Stencil {
     int4 rows[kMaxRows];  // (o1, o2, o3, xr), nearest rows first
 };
 
+// Per-job parameters of a batched run (independent DBSCAN jobs concatenated into
+// one pipeline).  Kernels take a null table in a single-job run.  Cell keys of
+// job j are key_base + the job's own cell key, so jobs never share a cell.
+struct JobDev {
+    long long off;                 // first point of the job in the concatenated input
+    long long n;                   // points of the job
+    float e2;                      // eps * eps (FP32)
+    int min_pts;
+    int list_cap;                  // neighbour-list entries recorded (min_pts - 1, 0 = none)
+    int linked;                    // same-cell-linked grid (cell units)
+    unsigned long long key_base;   // first composite cell key of the job
+    GridDev g;
+    const float *src;              // the job's coordinates (device), gathered into the batch
+    int32_t *nn_out;               // caller's outputs (device; may be null)
+    int32_t *ci_out;
+};
+
+// job of a point in concatenated input order (jobs sorted by offset)
+__device__ __forceinline__ int job_of_point(const JobDev *__restrict__ jobs, int n_jobs, long long o) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].off <= o) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 constexpr int kBlock = 256;
 constexpr int kMaxRowCells = 5;
 constexpr int kMaxListCap = 64;  // largest min_pts - 1 for which neighbour lists are kept
@@ -311,22 +339,31 @@ __device__ __forceinline__ void decode_key(K key, const GridDev &g, long long &x
 // are issued together.
 template <typename K>
 __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell_key, int64_t n_cells,
-                                                      GridDev g, const int4 *__restrict__ rows, int n_rows,
+                                                      GridDev g_one, const int4 *__restrict__ rows, int n_rows,
                                                       const K *__restrict__ hkeys, const int32_t *__restrict__ hvals,
-                                                      unsigned long long mask, int2 *__restrict__ nbr) {
+                                                      unsigned long long mask, int2 *__restrict__ nbr,
+                                                      const JobDev *__restrict__ jobs,
+                                                      const int32_t *__restrict__ cell_job) {
     __shared__ int4 s_rows[kMaxRows];
     for (int r = threadIdx.x; r < n_rows; r += blockDim.x) s_rows[r] = rows[r];
     __syncthreads();
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n_cells) return;
+    unsigned long long key_base = 0;
+    GridDev g = g_one;
+    if (jobs) {
+        const JobDev &J = jobs[cell_job[c]];
+        g = J.g;
+        key_base = J.key_base;
+    }
     long long cc[kMaxGridDims];
-    decode_key<K>(cell_key[c], g, cc);
+    decode_key<K>((K)((unsigned long long)cell_key[c] - key_base), g, cc);
     int2 *out = nbr + c * n_rows;
     for (int r = 0; r < n_rows; ++r) {
         const int4 row = s_rows[r];
         const int off[kMaxGridDims] = {0, row.x, row.y, row.z};
         bool in = true;
-        unsigned long long base = 0;
+        unsigned long long base = key_base;
 #pragma unroll
         for (int a = 1; a < kMaxGridDims; ++a) {
             if (a < g.k) {
@@ -445,7 +482,8 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts,
     int dense_skip, int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap,
-    unsigned long long *__restrict__ pair_counter) {
+    int list_stride, unsigned long long *__restrict__ pair_counter, const JobDev *__restrict__ jobs,
+    const int32_t *__restrict__ cell_job) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ RowTable s_rows[kWarpsPerBlock];
@@ -458,9 +496,16 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     const int cell = item.x, p0 = item.y;
     const int cs = cell_start[cell], ce = cell_start[cell + 1];
     const int cnt = min(kTile, ce - p0);
+    if (jobs) {
+        const JobDev &J = jobs[cell_job[cell]];
+        e2 = J.e2;
+        min_pts = J.min_pts;
+        dense_skip = J.linked;
+        list_cap = J.list_cap;
+    }
     // lists of up to kSmemListCap entries are gathered in shared memory and written
     // out only for the points that end below min_pts; longer ones go straight out
-    const bool smem_list = list_cap <= kSmemListCap;
+    const bool smem_list = list_stride <= kSmemListCap;
     int *sl = s_list[wib];
     if (EARLY && dense_skip && ce - cs >= min_pts) {
         if (lane < cnt) nn_sorted[p0 + lane] = ce - cs;
@@ -502,7 +547,7 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
                 const int slot = ck + __popc(m & lanemask_lt());
                 if (hit && slot < list_cap) {
                     if (smem_list) sl[k * kSmemListCap + slot] = j;
-                    else nbr_list[(int64_t)(p0 + k) * list_cap + slot] = j;
+                    else nbr_list[(int64_t)(p0 + k) * list_stride + slot] = j;
                 }
             }
             __syncwarp();
@@ -522,7 +567,7 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         __syncwarp();
         if (lane < cnt && mine < min_pts) {
             const int len = min(mine, list_cap);
-            for (int q = 0; q < len; ++q) nbr_list[(int64_t)(p0 + lane) * list_cap + q] = sl[lane * kSmemListCap + q];
+            for (int q = 0; q < len; ++q) nbr_list[(int64_t)(p0 + lane) * list_stride + q] = sl[lane * kSmemListCap + q];
         }
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
@@ -535,9 +580,11 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
 __global__ void core_flags_kernel(const int32_t *__restrict__ nn_sorted, int64_t nv, int64_t n, int min_pts,
                                   const int32_t *__restrict__ perm, const int32_t *__restrict__ pcell,
                                   uint8_t *__restrict__ core_sorted, uint8_t *__restrict__ cell_has_core,
-                                  uint32_t *__restrict__ core_bits) {
+                                  uint32_t *__restrict__ core_bits, const JobDev *__restrict__ jobs,
+                                  const int32_t *__restrict__ cell_job, int n_jobs) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
+    if (jobs) min_pts = jobs[s < nv ? cell_job[pcell[s]] : job_of_point(jobs, n_jobs, perm[s])].min_pts;
     bool core;
     if (s < nv) {
         core = nn_sorted[s] >= min_pts;
@@ -569,9 +616,18 @@ __device__ __forceinline__ int32_t core_rank(const uint32_t *__restrict__ bits, 
 
 // nn in input order (the caller's nn output)
 __global__ void scatter_nn_kernel(const int32_t *__restrict__ nn_sorted, int64_t nv, int64_t n,
-                                  const int32_t *__restrict__ perm, int32_t *__restrict__ out) {
+                                  const int32_t *__restrict__ perm, int32_t *__restrict__ out,
+                                  const JobDev *__restrict__ jobs, int n_jobs) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < n) out[perm[s]] = s < nv ? nn_sorted[s] : 0;
+    if (s >= n) return;
+    const int32_t o = perm[s];
+    const int32_t v = s < nv ? nn_sorted[s] : 0;
+    if (jobs) {
+        const JobDev &J = jobs[job_of_point(jobs, n_jobs, o)];
+        if (J.nn_out) J.nn_out[o - J.off] = v;
+    } else {
+        out[o] = v;
+    }
 }
 
 __global__ void iota_kernel(int32_t *__restrict__ a, int64_t n) {
@@ -666,18 +722,26 @@ __device__ __forceinline__ void load_first_cores(const float *__restrict__ xs, c
 
 template <int D, typename K>
 __global__ void __launch_bounds__(kBlock) union_near_kernel(
-    int64_t n_cells, GridDev g, const K *__restrict__ cell_key, const int32_t *__restrict__ cell_start,
+    int64_t n_cells, GridDev g_one, const K *__restrict__ cell_key, const int32_t *__restrict__ cell_start,
     const K *__restrict__ hkeys, const int32_t *__restrict__ hvals, unsigned long long mask,
     const float *__restrict__ xs, float e2, const uint8_t *__restrict__ core_sorted,
     const uint8_t *__restrict__ cell_has_core, int32_t *parent, unsigned long long *__restrict__ pair_counter,
-    int *err) {
+    int *err, const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned pairs = 0;
     if (idx < n_cells && cell_has_core[idx]) {
         const int A = (int)idx;
         const unsigned long long key = (unsigned long long)cell_key[A];
+        GridDev g = g_one;
+        unsigned long long key_base = 0;
+        if (jobs) {
+            const JobDev &J = jobs[cell_job[A]];
+            g = J.g;
+            e2 = J.e2;
+            key_base = J.key_base;
+        }
         long long cc[kMaxGridDims];
-        decode_key<K>(cell_key[A], g, cc);
+        decode_key<K>((K)(key - key_base), g, cc);
         int nb[3] = {-1, -1, -1};
         if (cc[0] + 1 < g.g[0] && A + 1 < n_cells && (unsigned long long)cell_key[A + 1] == key + 1ull) nb[0] = A + 1;
         if (g.k >= 2 && cc[1] + 1 < g.g[1]) nb[1] = hash_find(hkeys, hvals, mask, key + g.stride[1]);
@@ -729,7 +793,7 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
     int64_t n_cells, const int32_t *__restrict__ cell_start, const int2 *__restrict__ nbr, int n_rows,
     const float *__restrict__ xs, float e2, const uint8_t *__restrict__ core_sorted,
     const uint8_t *__restrict__ cell_has_core, int32_t *parent, unsigned long long *__restrict__ pair_counter,
-    int *err) {
+    int *err, const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ RowTable s_rows[kWarpsPerBlock];
@@ -739,6 +803,7 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
     if (A64 >= n_cells) return;
     const int A = (int)A64;
     if (!cell_has_core[A]) return;
+    if (jobs) e2 = jobs[cell_job[A]].e2;
     RowTable &rt = s_rows[wib];
     int *sb = s_b[wib];
     const int total = gather_rows<true>(nbr + (int64_t)A * n_rows, n_rows, cell_start, A + 1, rt, lane);
@@ -826,7 +891,8 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2,
     const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core,
-    int32_t *parent, unsigned long long *__restrict__ pair_counter, int *err) {
+    int32_t *parent, unsigned long long *__restrict__ pair_counter, int *err, const JobDev *__restrict__ jobs,
+    const int32_t *__restrict__ cell_job) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ int s_idx[kWarpsPerBlock][kTile];
@@ -838,6 +904,7 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     const int2 item = items[item_id];
     const int A = item.x, p0 = item.y;
     if (!cell_has_core[A]) return;
+    if (jobs) e2 = jobs[cell_job[A]].e2;
     const int cnt = min(kTile, cell_start[A + 1] - p0);
     float *si = s_i[wib];
     int *sidx = s_idx[wib];
@@ -927,7 +994,8 @@ __global__ void flatten_kernel(int32_t *parent, int64_t n_units, int *err) {
 __global__ void core_ids_kernel(int64_t nv, const uint8_t *__restrict__ core_sorted,
                                 const int32_t *__restrict__ pcell, int cell_units,
                                 const int32_t *__restrict__ parent, const int32_t *__restrict__ comp_min,
-                                int32_t *__restrict__ ci_sorted, unsigned long long *__restrict__ counters) {
+                                int32_t *__restrict__ ci_sorted, unsigned long long *__restrict__ counters,
+                                const int32_t *__restrict__ cell_job, unsigned long long *__restrict__ job_counters) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned roots = 0;
     if (s < nv) {
@@ -935,7 +1003,10 @@ __global__ void core_ids_kernel(int64_t nv, const uint8_t *__restrict__ core_sor
             const int u = cell_units ? pcell[s] : (int)s;
             const int root = parent[u];
             ci_sorted[s] = comp_min[root];
-            if (!cell_units && root == (int)s) roots = 1;
+            if (!cell_units && root == (int)s) {
+                if (job_counters) atomicAdd(job_counters + 4 * cell_job[pcell[s]], 1ull);
+                else roots = 1;
+            }
         } else {
             ci_sorted[s] = kNoCluster;
         }
@@ -947,14 +1018,18 @@ __global__ void core_ids_kernel(int64_t nv, const uint8_t *__restrict__ core_sor
 // clusters over cells + the id of every cell's component
 __global__ void cell_ids_kernel(int64_t n_cells, const uint8_t *__restrict__ cell_has_core,
                                 const int32_t *__restrict__ parent, const int32_t *__restrict__ comp_min,
-                                int32_t *__restrict__ cell_cid, unsigned long long *__restrict__ counters) {
+                                int32_t *__restrict__ cell_cid, unsigned long long *__restrict__ counters,
+                                const int32_t *__restrict__ cell_job, unsigned long long *__restrict__ job_counters) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned roots = 0;
     if (c < n_cells) {
         if (cell_has_core[c]) {
             const int root = parent[c];
             cell_cid[c] = comp_min[root];
-            if (root == (int)c) roots = 1;
+            if (root == (int)c) {
+                if (job_counters) atomicAdd(job_counters + 4 * cell_job[c], 1ull);
+                else roots = 1;
+            }
         } else {
             cell_cid[c] = kNoCluster;
         }
@@ -1117,17 +1192,17 @@ __global__ void __launch_bounds__(kBlock) border_kernel(
 // minimum id over the cores among them -- no second stencil scan.
 // ---------------------------------------------------------------------------
 __global__ void border_list_kernel(int64_t nv, const int32_t *__restrict__ nn_sorted,
-                                   const int32_t *__restrict__ nbr_list, int list_cap,
+                                   const int32_t *__restrict__ nbr_list, int list_stride,
                                    const uint8_t *__restrict__ core_sorted, int cell_units,
                                    const int32_t *__restrict__ pcell, const int32_t *__restrict__ cell_cid,
                                    int32_t *__restrict__ ci_sorted, unsigned long long *__restrict__ pair_counter) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned looked = 0;
     if (s < nv && !core_sorted[s]) {
-        const int cnt = min(nn_sorted[s], list_cap);
+        const int cnt = min(nn_sorted[s], list_stride);
         int best = kNoCluster;
         for (int q = 0; q < cnt; ++q) {
-            const int j = nbr_list[s * list_cap + q];
+            const int j = nbr_list[s * list_stride + q];
             if (core_sorted[j]) best = min(best, cell_units ? cell_cid[pcell[j]] : ci_sorted[j]);
         }
         looked = (unsigned)cnt;
@@ -1144,7 +1219,8 @@ __global__ void border_list_kernel(int64_t nv, const int32_t *__restrict__ nn_so
 __global__ void output_ci_kernel(const int32_t *__restrict__ ci_sorted, int64_t nv, int64_t n,
                                  const int32_t *__restrict__ perm, const uint32_t *__restrict__ core_bits,
                                  const uint32_t *__restrict__ core_prefix, int32_t *__restrict__ out,
-                                 unsigned long long *__restrict__ counters) {
+                                 unsigned long long *__restrict__ counters, const JobDev *__restrict__ jobs,
+                                 int n_jobs, unsigned long long *__restrict__ job_counters) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned noise = 0, roots = 0;
     if (s < n) {
@@ -1159,7 +1235,19 @@ __global__ void output_ci_kernel(const int32_t *__restrict__ ci_sorted, int64_t 
             v = kNoCluster;
         }
         noise = v == kNoCluster;
-        if (out) out[o] = v;
+        if (jobs) {
+            // ids are ranks among all cores of the batch: make them ranks within the job
+            const int j = job_of_point(jobs, n_jobs, o);
+            const JobDev &J = jobs[j];
+            if (v != kNoCluster) v -= core_rank(core_bits, core_prefix, (int32_t)J.off);
+            if (J.ci_out) J.ci_out[o - J.off] = v;
+            if (noise) atomicAdd(job_counters + 4 * j + 1, 1ull);
+            if (roots) atomicAdd(job_counters + 4 * j, 1ull);
+            noise = 0;
+            roots = 0;
+        } else if (out) {
+            out[o] = v;
+        }
     }
     noise = __reduce_add_sync(kFull, noise);
     roots = __reduce_add_sync(kFull, roots);
@@ -1179,6 +1267,139 @@ __global__ void labels_kernel(const int32_t *__restrict__ ci_sorted, int64_t nv,
     if (!is_core_o(core_bits, o)) return;
     const int32_t r = core_rank(core_bits, core_prefix, o);
     labels[r] = s < nv ? ci_sorted[s] : r;
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched runs: per-job bounding boxes, the concatenation of the jobs'
+// coordinates, composite cell keys and the cell -> job map.  blockIdx.y is the job.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(kBlock) gather_jobs_kernel(const JobDev *__restrict__ jobs,
+                                                             float *__restrict__ coords) {
+    const JobDev &J = jobs[blockIdx.y];
+    const int64_t total = J.n * D;
+    float *dst = coords + J.off * D;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = J.src[i];
+}
+
+__global__ void bbox_batch_init_kernel(int *lo_hi, int d, int n_jobs, unsigned long long *n_invalid) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < (int64_t)n_jobs * d) {
+        const int64_t j = i / d, k = i - j * d;
+        lo_hi[j * 2 * d + k] = 0x7fffffff;
+        lo_hi[j * 2 * d + d + k] = (int)0x80000000;
+    }
+    if (i < n_jobs) n_invalid[i] = 0ull;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kBlock) bbox_batch_kernel(const float *__restrict__ coords,
+                                                            const JobDev *__restrict__ jobs, int *lo_hi,
+                                                            unsigned long long *n_invalid) {
+    const int j = blockIdx.y;
+    const JobDev &J = jobs[j];
+    int lo[D], hi[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        lo[k] = 0x7fffffff;
+        hi[k] = (int)0x80000000;
+    }
+    unsigned bad = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < J.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float *p = coords + (J.off + i) * D;
+        float x[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) x[k] = p[k];
+        bool ok = x[0] != FLT_MAX;
+#pragma unroll
+        for (int k = 0; k < D; ++k) ok = ok && isfinite(x[k]);
+        if (!ok) {
+            ++bad;
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const int v = ordered_int(x[k]);
+            lo[k] = min(lo[k], v);
+            hi[k] = max(hi[k], v);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = min(lo[k], __shfl_xor_sync(kFull, lo[k], o));
+            hi[k] = max(hi[k], __shfl_xor_sync(kFull, hi[k], o));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(kFull, bad, o);
+    if ((threadIdx.x & 31) == 0) {
+        int *lh = lo_hi + (int64_t)j * 2 * D;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            if (lo[k] != 0x7fffffff) atomicMin(lh + k, lo[k]);
+            if (hi[k] != (int)0x80000000) atomicMax(lh + D + k, hi[k]);
+        }
+        if (bad) atomicAdd(n_invalid + j, (unsigned long long)bad);
+    }
+}
+
+template <int D, typename K>
+__global__ void __launch_bounds__(kBlock) key_batch_kernel(const float *__restrict__ coords,
+                                                           const JobDev *__restrict__ jobs, K invalid_key,
+                                                           K *__restrict__ keys, int32_t *__restrict__ ids) {
+    const JobDev &J = jobs[blockIdx.y];
+    const GridDev g = J.g;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < J.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = J.off + i;
+        const float *p = coords + o * D;
+        K key = invalid_key;
+        if (point_valid<D>(p)) {
+            unsigned long long kk = J.key_base;
+#pragma unroll
+            for (int a = 0; a < kMaxGridDims; ++a)
+                if (a < g.k) kk += (unsigned long long)cell_coord(g, a, p[g.dim[a]]) * g.stride[a];
+            key = (K)kk;
+        }
+        keys[o] = key;
+        ids[o] = (int32_t)o;
+    }
+}
+
+// job of every cell: the last job whose key range starts at or below the cell key
+// (every job of a pipeline owns a non-empty key range, so the bases increase)
+template <typename K>
+__global__ void cell_job_kernel(const K *__restrict__ cell_key, int64_t n_cells, const JobDev *__restrict__ jobs,
+                                int n_jobs, int32_t *__restrict__ cell_job) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    const unsigned long long key = (unsigned long long)cell_key[c];
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].key_base <= key) lo = mid;
+        else hi = mid - 1;
+    }
+    cell_job[c] = lo;
+}
+
+// cores of every job: rank of the job's end minus rank of its start
+__global__ void job_cores_kernel(const JobDev *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ core_bits,
+                                 const uint32_t *__restrict__ core_prefix, int64_t n_total,
+                                 unsigned long long *__restrict__ job_counters) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_jobs) return;
+    const JobDev &J = jobs[j];
+    const int64_t end = J.off + J.n;
+    const int32_t r0 = core_rank(core_bits, core_prefix, (int32_t)J.off);
+    const int32_t r1 = end < n_total ? core_rank(core_bits, core_prefix, (int32_t)end)
+                                     : (int32_t)(core_prefix[(n_total - 1) >> 5] +
+                                                 __popc(core_bits[(n_total - 1) >> 5] &
+                                                        (0xffffffffu >> (31 - ((n_total - 1) & 31)))));
+    job_counters[4 * j + 2] = (unsigned long long)(r1 - r0);
 }
 
 }  // namespace ndb

@@ -41,6 +41,7 @@ EXPORTED = (
     "ndb_b200_classify",
     "ndb_b200_assign_labels",
     "ndb_b200_run",
+    "ndb_b200_run_batched",
     "ndb_b200_cluster_label",
     "ndb_b200_get_stats",
     "ndb_b200_strerror",
@@ -54,6 +55,14 @@ class NdbResult(ctypes.Structure):
 
     _fields_ = [("clusters", ctypes.c_int32), ("noise", ctypes.c_int32),
                 ("core_count", ctypes.c_int32), ("n", ctypes.c_int32)]
+
+
+class NdbJob(ctypes.Structure):
+    """ndb_job: one independent problem of ndb_b200_run_batched."""
+
+    _fields_ = [("coords", ctypes.c_void_p), ("n", ctypes.c_int64), ("d", ctypes.c_int32),
+                ("eps", ctypes.c_float), ("min_pts", ctypes.c_int32), ("nn_out", ctypes.c_void_p),
+                ("cluster_index_out", ctypes.c_void_p), ("result", NdbResult), ("status", ctypes.c_int32)]
 
 
 class NdbStats(ctypes.Structure):
@@ -121,6 +130,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
                                      ctypes.c_float, ctypes.c_int32, ctypes.c_uint32, i32p, i32p,
                                      ctypes.POINTER(NdbResult)]
+        lib.ndb_b200_run_batched.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbJob), ctypes.c_int64,
+                                             ctypes.c_uint32]
         lib.ndb_b200_cluster_label.argtypes = [ctypes.c_void_p, i32p, ctypes.c_int64]
         lib.ndb_b200_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbStats)]
         lib.ndb_b200_strerror.argtypes = [ctypes.c_int]
@@ -129,7 +140,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_last_cuda_error.restype = ctypes.c_char_p
         lib.ndb_b200_version.restype = ctypes.c_char_p
         for name in ("ndb_b200_create", "ndb_b200_destroy", "ndb_b200_set_stream", "ndb_b200_classify",
-                     "ndb_b200_assign_labels", "ndb_b200_run", "ndb_b200_cluster_label",
+                     "ndb_b200_assign_labels", "ndb_b200_run", "ndb_b200_run_batched", "ndb_b200_cluster_label",
                      "ndb_b200_get_stats"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib

@@ -122,6 +122,68 @@ def config5(n: int = 100_000_000, seed: int = 5, n_gauss: int = 10_000, n_filame
     return Workload("skew-2d-100m", _finish(rng, blocks), 0.5, 4)
 
 
+@dataclasses.dataclass(frozen=True)
+class BatchJob:
+    coords: np.ndarray  # float32, n x d
+    eps: float
+    min_pts: int
+
+    @property
+    def n(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def d(self) -> int:
+        return int(self.coords.shape[1])
+
+
+def _eps_4nn(rng: np.random.Generator, pts: np.ndarray) -> float:
+    """90th percentile, over a 1% sample (at least 10 points), of the distance from
+    each sampled point to its 4th nearest neighbour in the whole job."""
+    from scipy.spatial import cKDTree
+
+    n = pts.shape[0]
+    m = min(n, max(10, n // 100))
+    idx = rng.choice(n, m, replace=False)
+    dist, _ = cKDTree(pts).query(pts[idx], k=5)  # k=5: the point itself is the first hit
+    return float(np.percentile(dist[:, 4], 90))
+
+
+def _one_job(args) -> BatchJob:
+    seq, n_min, n_max, dims = args
+    rng = np.random.Generator(np.random.PCG64(seq))
+    n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+    d = int(dims[rng.integers(0, len(dims))])
+    k = int(rng.integers(5, 51))
+    n_noise = int(round(n * 0.05))
+    centers = rng.uniform(0.0, 100.0, (k, d))
+    sig = rng.uniform(0.5, 2.0, k)
+    pts = gaussian_mixture(rng, n - n_noise, centers, sig)
+    noise = rng.uniform(0.0, 100.0, (n_noise, d))
+    x = _finish(rng, [pts, noise])
+    return BatchJob(x, _eps_4nn(rng, x.astype(np.float64)), 2 * d)
+
+
+def config4(n_jobs: int = 4096, seed: int = 4, n_min: int = 1_000, n_max: int = 200_000,
+            dims: tuple = (2, 3, 8, 16), workers: int | None = None) -> list[BatchJob]:
+    """4,096 independent jobs: n log-uniform in [1,000, 200,000], d uniform in
+    {2,3,8,16}, each a mixture of 5-50 isotropic Gaussians (centres U[0,100]^d,
+    sigma U[0.5,2]) + 5% uniform noise; eps = 90th percentile of the 4-NN distance
+    over a 1% sample; minPts = 2d.  Job j draws from the j-th child of
+    SeedSequence(seed), so any prefix of the batch is reproducible alone."""
+    seqs = np.random.SeedSequence(seed).spawn(n_jobs)
+    args = [(s, n_min, n_max, tuple(dims)) for s in seqs]
+    if workers is None:
+        import os
+        workers = min(len(os.sched_getaffinity(0)), 32) if n_jobs >= 64 else 1
+    if workers <= 1:
+        return [_one_job(a) for a in args]
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(workers) as pool:  # spawn: callers may already hold a CUDA context
+        return pool.map(_one_job, args, chunksize=max(1, n_jobs // (8 * workers)))
+
+
 CONFIGS = {1: config1, 2: config2, 3: config3, 5: config5}
 
 
