@@ -43,12 +43,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", type=int, default=2, help="benchmark configuration (1, 2, 3 or 5)")
+    ap.add_argument("--config", type=int, default=2, help="benchmark configuration (1..5; 4 is the batched one)")
     ap.add_argument("--n", type=int, default=None, help="override n (smaller runs for profiling)")
     ap.add_argument("--full-count", action="store_true", help="exact neighbour counts (no early exit)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=50_000, help="points in the bounded CPU sample")
+    ap.add_argument("--jobs", type=int, default=4096, help="jobs of the batched configuration 4")
+    ap.add_argument("--no-plain", action="store_true", help="configuration 4: skip the one-call-per-job form")
     return ap.parse_args()
 
 
@@ -175,6 +177,50 @@ def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1,
     }
 
 
+def batch_sample(pkg, n_jobs: int = 24, n_cap: int = 40_000):
+    """The bounded CPU sample of the batched configuration: the first n_jobs jobs of
+    the 4,096-job batch (same generator, same seed) whose n is at most n_cap."""
+    jobs = pkg.synthetic.config4(n_jobs=128)
+    return [j for j in jobs if j.n <= n_cap][:n_jobs]
+
+
+def cpu_reference_batch(pkg, threads: int, steps: int = 1, warmup: int = 0):
+    import oracle
+
+    if not oracle.have_ref():
+        try:
+            oracle.build("/root/reference" if os.path.isdir("/root/reference") else None)
+        except Exception:
+            pass
+    jobs = batch_sample(pkg)
+    pts = sum(j.n for j in jobs)
+    times = []
+    kind = "reference" if oracle.have_ref() else "port"
+    for i in range(warmup + steps):
+        t = 0.0
+        for j in jobs:
+            if kind == "reference":
+                t += oracle.run_ref(j.coords, j.eps, j.min_pts, threads=threads)[3]["total_ms"] / 1000.0
+            else:
+                t0 = time.perf_counter()
+                oracle.grid(j.coords, j.eps, j.min_pts)
+                t += time.perf_counter() - t0
+        if i >= warmup:
+            times.append(t)
+    per_step = sum(times) / len(times)
+    cores = threads if kind == "reference" else oracle.threads()
+    return {
+        "value": pts / per_step, "unit": UNIT, "cores": cores, "kind": kind,
+        "sample": (f"the first {len(jobs)} jobs with n <= 40,000 of the 4,096-job batch ({pts} points, "
+                   f"d in {sorted({j.d for j in jobs})}); "
+                   f"{'reference OpenMP data_process (oracle/_ref)' if kind == 'reference' else 'oracle grid port'}"
+                   f", one job after another, {cores} threads, {per_step:.2f} s; the reference is O(n^2) per job, "
+                   f"so on the full batch (mean n 37k, up to 200k) its rate is lower"),
+        "seconds_per_step": per_step,
+        "workload": "batched-4096-jobs",
+    }
+
+
 def run_reference_arm(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -182,13 +228,16 @@ def run_reference_arm(args):
     import importlib
     pkg = importlib.import_module("nextdbscan-exa_b200")
     threads = os.cpu_count() or 1
-    cb = cpu_reference(pkg, args.config, args.cpu_sample, threads, steps=args.steps, warmup=args.warmup)
+    if args.config == 4:
+        cb = cpu_reference_batch(pkg, threads, steps=args.steps, warmup=args.warmup)
+    else:
+        cb = cpu_reference(pkg, args.config, args.cpu_sample, threads, steps=args.steps, warmup=args.warmup)
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["seconds_per_step"] * 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator, benchmark distribution)",
-        "config": {"workload": cb["workload"], "sample_n": args.cpu_sample, "parallelism": "host OpenMP"},
+        "config": {"workload": cb["workload"], "sample": cb["sample"], "parallelism": "host OpenMP"},
         "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -252,6 +301,35 @@ def run_ours(args):
     total_ms = max_over_ranks(sum(step_ms), world)
     value = world * n * args.steps / (total_ms / 1000.0)
 
+    # d >= 8: the plain GPU form (exact FP32 count kernel) and the tensor-core filtered
+    # form beside the default (the library picks between them by tile fill)
+    forms = {}
+    if d >= 8 and not args.no_plain:
+        ci_chosen = ci.cpu().numpy()
+        for name, kw in (("exact_fp32_count", {"exact_count": True}), ("tensor_filter_count", {"tensor_filter": True})):
+            def form_step():
+                return ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(),
+                                      full_count=full, **kw)
+            form_step()
+            torch.cuda.synchronize()
+            f_ms = []
+            for _ in range(args.steps):
+                flush.fill_(1)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                form_step()
+                e1.record(stream)
+                e1.synchronize()
+                f_ms.append(e0.elapsed_time(e1))
+            fs = ctx.stats()
+            fv = n * len(f_ms) / (sum(f_ms) / 1000.0)
+            forms[name] = {"value": fv, "unit": UNIT, "ms_per_step": sum(f_ms) / len(f_ms),
+                           "count_kernel_ms": fs["ms_count_kernel"], "tensor_filter": bool(fs["tensor_filter"]),
+                           "band_pairs": fs["band_pairs"], "filtered_pairs": fs["count_pairs"],
+                           "identical_cluster_ids": bool(np.array_equal(ci.cpu().numpy(), ci_chosen))}
+        forms["chosen_over_plain"] = value / world / forms["exact_fp32_count"]["value"]
+
     # end to end through the public API: pinned host input -> device -> pinned host labels
     e2e = None
     if not args.no_e2e:
@@ -289,7 +367,7 @@ def run_ours(args):
     }
     s0 = stats[-1]
     dominant = max(kern, key=kern.get)
-    roof = roofline(dominant, kern[dominant], s0, n, d, hbm_peak, peak_src, clk_sum)
+    roof = roofline(dominant, kern[dominant], s0, n, hbm_peak, peak_src, clk_sum)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -308,7 +386,9 @@ def run_ours(args):
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk_sum,
-            "gpu_launches": launches * args.steps,
+            "gpu_launches": launches * args.steps, "count_forms": forms or None,
+            "tensor_filter": {"used": bool(s0["tensor_filter"]), "band_pairs": s0["band_pairs"],
+                              "filtered_pairs": s0["count_pairs"]},
             "result": {"clusters": res.clusters, "noise": res.noise, "core_count": res.core_count},
             "phases_ms": {k: round(statistics.mean(s[k] for s in stats), 4)
                           for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
@@ -326,24 +406,209 @@ def run_ours(args):
     return 0
 
 
+def run_ours_batch(args):
+    """Configuration 4: 4,096 independent jobs per step through ndb_b200_run_batched
+    (the chosen form), beside the same jobs as one ndb_b200_run call each (the
+    plain GPU form)."""
+    import importlib
+
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    pkg = importlib.import_module("nextdbscan-exa_b200")
+    lib = pkg.lib
+    jobs = pkg.synthetic.config4(n_jobs=args.jobs)
+    nj = len(jobs)
+    sizes = np.array([j.n for j in jobs], np.int64)
+    dims = np.array([j.d for j in jobs], np.int64)
+    total = int(sizes.sum())
+    foff = np.concatenate([[0], np.cumsum(sizes * dims)])
+    poff = np.concatenate([[0], np.cumsum(sizes)])
+    flat = np.empty(int(foff[-1]), np.float32)
+    for k, j in enumerate(jobs):
+        flat[foff[k]:foff[k + 1]] = j.coords.ravel()
+    stream = torch.cuda.current_stream()
+    ctx = pkg.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    x = torch.from_numpy(flat).cuda()
+    nn = torch.empty(total, dtype=torch.int32, device="cuda")
+    ci = torch.empty(total, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def job_table(xp, nnp, cip):
+        arr = (lib.NdbJob * nj)()
+        for k, j in enumerate(jobs):
+            arr[k].coords = xp + 4 * int(foff[k])
+            arr[k].n, arr[k].d, arr[k].eps, arr[k].min_pts = j.n, j.d, j.eps, j.min_pts
+            arr[k].nn_out = nnp + 4 * int(poff[k])
+            arr[k].cluster_index_out = cip + 4 * int(poff[k])
+        return arr
+
+    full = lib.FLAG_FULL_COUNT if args.full_count else 0
+    dev_jobs = job_table(x.data_ptr(), nn.data_ptr(), ci.data_ptr())
+    torch.cuda.synchronize()
+
+    def step():
+        st = ctx.run_batched_jobs(dev_jobs, nj, lib.FLAG_DEVICE_PTRS | full)
+        if st != 0:
+            raise lib.NdbError(st, "ndb_b200_run_batched")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    step_ms, stats = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            stats.append(ctx.stats())
+    torch.cuda.synchronize()
+    barrier(world)
+    total_ms = max_over_ranks(sum(step_ms), world)
+    value = world * total * args.steps / (total_ms / 1000.0)
+    h_ci = ci.cpu().numpy()
+    clusters = sum(int(dev_jobs[k].result.clusters) for k in range(nj))
+    noise = sum(int(dev_jobs[k].result.noise) for k in range(nj))
+    cores = sum(int(dev_jobs[k].result.core_count) for k in range(nj))
+
+    # the plain GPU form: the same jobs, one ndb_b200_run call each
+    plain = None
+    if not args.no_plain:
+        def plain_step():
+            for k, j in enumerate(jobs):
+                ctx.run_device(x.data_ptr() + 4 * int(foff[k]), j.n, j.d, j.eps, j.min_pts,
+                               nn.data_ptr() + 4 * int(poff[k]), ci.data_ptr() + 4 * int(poff[k]),
+                               full_count=bool(full))
+        plain_step()
+        torch.cuda.synchronize()
+        p_ms = []
+        for _ in range(max(1, min(args.steps, 2))):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plain_step()
+            e1.record(stream)
+            e1.synchronize()
+            p_ms.append(e0.elapsed_time(e1))
+        same = bool(np.array_equal(ci.cpu().numpy(), h_ci))
+        pv = total * len(p_ms) / (sum(p_ms) / 1000.0)
+        plain = {"value": pv, "unit": UNIT, "ms_per_step": sum(p_ms) / len(p_ms),
+                 "form": "one ndb_b200_run call per job, device-resident inputs",
+                 "chosen_over_plain": value / world / pv, "identical_cluster_ids": same}
+
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.from_numpy(flat).pin_memory()
+        hnn = torch.empty(total, dtype=torch.int32).pin_memory()
+        hci = torch.empty(total, dtype=torch.int32).pin_memory()
+        host_jobs = job_table(hx.data_ptr(), hnn.data_ptr(), hci.data_ptr())
+
+        def e2e_step():
+            st = ctx.run_batched_jobs(host_jobs, nj, full)
+            if st != 0:
+                raise lib.NdbError(st, "ndb_b200_run_batched")
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        e_ms = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            e2e_step()
+            e1.record(stream)
+            e1.synchronize()
+            e_ms.append(e0.elapsed_time(e1))
+        e_total = max_over_ranks(sum(e_ms), world)
+        assert np.array_equal(hci.numpy(), h_ci), "host-buffer batch differs from the device-buffer batch"
+        e2e = {"value": world * total * args.steps / (e_total / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": int(flat.nbytes), "d2h_bytes_per_step": 2 * total * 4}
+
+    hbm_peak, peak_src = peaks()
+    clk_sum = clk.summary()
+    kern = {
+        "count_kernel": statistics.mean(s["ms_count_kernel"] for s in stats),
+        "union_kernel": statistics.mean(s["ms_union_kernel"] for s in stats),
+        "border_kernel": statistics.mean(s["ms_border_kernel"] for s in stats),
+        "radix_sort": statistics.mean(s["ms_sort_kernels"] for s in stats),
+    }
+    s0 = stats[-1]
+    dominant = max(kern, key=kern.get)
+    roof = roofline(dominant, kern[dominant], s0, total, hbm_peak, peak_src, clk_sum)
+    roof["note"] = "summed over the pipelines of one batched call (one per dimensionality)"
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference_batch(pkg, os.cpu_count() or 1)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator with the benchmark's distribution)",
+            "config": {"workload": "batched-4096-jobs", "jobs": nj, "points": total,
+                       "points_by_d": {int(d): int(sizes[dims == d].sum()) for d in np.unique(dims)},
+                       "eps": "per job: 90th percentile of the 4-NN distance over a 1% sample",
+                       "min_pts": "2d", "form": "ndb_b200_run_batched, device-resident inputs",
+                       "counts": "exact" if full else "early-exit at minPts (exact core flags and labels)",
+                       "l2": "flushed between timed steps (256 MB write); inputs 4.4 GB",
+                       "parallelism": f"{world} independent replica(s), one per GPU"},
+            "e2e": e2e, "plain_gpu_form": plain, "roofline": roof, "cpu_baseline": cpu, "clocks": clk_sum,
+            "gpu_launches": count_launches(s0) * args.steps,
+            "result": {"clusters": clusters, "noise": noise, "core_count": cores},
+            "phases_ms": {k: round(statistics.mean(s[k] for s in stats), 4)
+                          for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
+            "kernels_ms": {k: round(v, 4) for k, v in kern.items()},
+            "pipelines": s0["pipelines"], "solo_jobs": s0["solo_jobs"],
+            "pairs": {"count": s0["count_pairs"], "union": s0["union_pairs"], "border": s0["border_pairs"]},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def count_launches(s) -> int:
     """Kernels of one job, as counted by the library at every launch site."""
     return int(s["kernel_launches"])
 
 
-def roofline(kind, ms, s, n, d, hbm_peak, peak_src, clk):
+def roofline(kind, ms, s, n, hbm_peak, peak_src, clk):
     """Algorithmic work of one launch / its device time."""
     if kind == "radix_sort":
         kb = s["key_bytes"]
         # per pass: upsweep reads keys; downsweep reads and writes (key, id)
-        per_pass = n * (kb + 2 * (kb + 4))
-        achieved = per_pass * s["sort_passes"] / (ms / 1000.0) / 1e9
+        per_pass = s["n_valid"] * (kb + 2 * (kb + 4))
+        achieved = per_pass * s["sort_passes"] / max(s.get("pipelines") or 1, 1) / (ms / 1000.0) / 1e9
         return {"kernel": "radix_sort (all passes)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
                 "peak_source": f"{peak_src} hbm_gbs"}
     pairs = {"count_kernel": s["count_pairs"], "union_kernel": s["union_pairs"],
              "border_kernel": s["border_pairs"]}[kind]
-    flops = pairs * 3 * d  # separately rounded sub, mul, add per dimension (no FMA credit)
+    pair_dims = {"count_kernel": s["count_pair_dims"], "union_kernel": s["union_pair_dims"],
+                 "border_kernel": s["border_pair_dims"]}[kind]
+    flops = pair_dims * 3  # separately rounded sub, mul, add per dimension (no FMA credit)
     achieved = flops / (ms / 1000.0) / 1e12
     mhz = clk.get("sm_mhz") or 1965.0
     peak = SM_COUNT * FP32_LANES_PER_SM * mhz * 1e6 / 1e12
@@ -358,6 +623,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.config == 4:
+        return run_ours_batch(args)
     return run_ours(args)
 
 

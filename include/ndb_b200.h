@@ -71,6 +71,10 @@ typedef enum ndb_status {
                                       upper bound on the cluster count. */
 #define NDB_FLAG_FULL_COUNT  0x2u  /* exact nn for every point (no early exit at min_pts) */
 #define NDB_FLAG_DEVICE_PTRS 0x4u  /* coords and outputs are device pointers */
+#define NDB_FLAG_EXACT_COUNT 0x8u  /* count with the exact FP32 kernel only, never the tensor-core
+                                    * filter (results are identical either way; this is the plain form) */
+#define NDB_FLAG_TENSOR_FILTER 0x10u /* d >= 8: count on the tensor-core filter whenever the input allows
+                                      * it, whatever the tile-fill heuristic would pick (results identical) */
 
 /* Mirrors nextdbscan::result (nextdbscan.h:43-48). */
 typedef struct ndb_result {
@@ -104,6 +108,13 @@ typedef struct ndb_stats {
     int32_t sort_passes;      /* radix passes (8 bits each) */
     int32_t key_bytes;        /* 4 or 8 */
     int32_t kernel_launches;  /* kernels launched by the last classify + assign_labels */
+    int32_t pipelines;        /* batched runs: pipelines built (one per d and chunk of jobs) */
+    int64_t count_pair_dims;  /* sum over pipelines of count_pairs x d (3 FP32 operations each) */
+    int64_t union_pair_dims;  /* the same for the union-find */
+    int64_t border_pair_dims; /* the same for the border assignment */
+    int32_t solo_jobs;        /* batched runs: jobs the pipelines could not take, run one call each */
+    int32_t tensor_filter;    /* 1 when the neighbour count ran on the tensor-core filter (d >= 8) */
+    int64_t band_pairs;       /* pairs inside the filter's guard band, rechecked with the exact predicate */
 } ndb_stats;
 
 typedef struct ndb_ctx ndb_ctx;

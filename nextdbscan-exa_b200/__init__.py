@@ -50,6 +50,13 @@ def _as_points(v_coord, n_dim: int | None = None) -> np.ndarray:
     return np.ascontiguousarray(a)
 
 
+def _flags(full_count: bool, approximate: bool, exact_count: bool = False, tensor_filter: bool = False,
+           device: bool = False) -> int:
+    return ((lib.FLAG_FULL_COUNT if full_count else 0) | (lib.FLAG_APPROXIMATE if approximate else 0)
+            | (lib.FLAG_EXACT_COUNT if exact_count else 0) | (lib.FLAG_TENSOR_FILTER if tensor_filter else 0)
+            | (lib.FLAG_DEVICE_PTRS if device else 0))
+
+
 class Context:
     """One libndb_b200 context (device buffers + stream) on one CUDA device."""
 
@@ -110,10 +117,11 @@ class Context:
         return ci, Result(res.clusters, res.noise, res.core_count, res.n)
 
     def run(self, coords, eps: float, min_pts: int, *, full_count: bool = False,
-            approximate: bool = False) -> tuple[np.ndarray, np.ndarray, Result]:
+            approximate: bool = False, exact_count: bool = False,
+            tensor_filter: bool = False) -> tuple[np.ndarray, np.ndarray, Result]:
         pts = _as_points(coords)
         n, d = pts.shape
-        flags = (lib.FLAG_FULL_COUNT if full_count else 0) | (lib.FLAG_APPROXIMATE if approximate else 0)
+        flags = _flags(full_count, approximate, exact_count, tensor_filter)
         nn = np.empty(n, dtype=np.int32)
         ci = np.empty(n, dtype=np.int32)
         res = lib.NdbResult()
@@ -126,9 +134,9 @@ class Context:
     # -- raw addresses: host (pageable or pinned) or, with device=True, device memory --
     def run_ptrs(self, coords_ptr: int, n: int, d: int, eps: float, min_pts: int, nn_ptr: int | None,
                  ci_ptr: int | None, *, device: bool, full_count: bool = False,
-                 approximate: bool = False) -> Result:
-        flags = (lib.FLAG_DEVICE_PTRS if device else 0) | (lib.FLAG_FULL_COUNT if full_count else 0) | (
-            lib.FLAG_APPROXIMATE if approximate else 0)
+                 approximate: bool = False, exact_count: bool = False,
+            tensor_filter: bool = False) -> Result:
+        flags = _flags(full_count, approximate, exact_count, tensor_filter, device)
         res = lib.NdbResult()
         st = self._lib.ndb_b200_run(self._h, ctypes.c_void_p(coords_ptr), n, d, ctypes.c_float(eps),
                                     int(min_pts), flags, ctypes.c_void_p(nn_ptr or 0),
@@ -139,9 +147,9 @@ class Context:
 
     # -- device buffers (addresses of device memory, e.g. torch tensors) ---
     def run_device(self, coords_ptr: int, n: int, d: int, eps: float, min_pts: int, nn_ptr: int | None,
-                   ci_ptr: int | None, *, full_count: bool = False, approximate: bool = False) -> Result:
-        flags = lib.FLAG_DEVICE_PTRS | (lib.FLAG_FULL_COUNT if full_count else 0) | (
-            lib.FLAG_APPROXIMATE if approximate else 0)
+                   ci_ptr: int | None, *, full_count: bool = False, approximate: bool = False,
+                   exact_count: bool = False, tensor_filter: bool = False) -> Result:
+        flags = _flags(full_count, approximate, exact_count, tensor_filter, True)
         res = lib.NdbResult()
         st = self._lib.ndb_b200_run(self._h, ctypes.c_void_p(coords_ptr), n, d, ctypes.c_float(eps),
                                     int(min_pts), flags, ctypes.c_void_p(nn_ptr or 0),
@@ -152,7 +160,8 @@ class Context:
 
     # -- many independent problems in one pipeline ----------------------------
     def run_batched(self, problems, *, full_count: bool = False, approximate: bool = False,
-                    want_nn: bool = True) -> list[tuple[np.ndarray | None, np.ndarray, Result]]:
+                    want_nn: bool = True, exact_count: bool = False,
+                    tensor_filter: bool = False) -> list[tuple[np.ndarray | None, np.ndarray, Result]]:
         """problems: iterable of (coords n x d, eps, min_pts).  Returns per problem
         (nn, cluster_index, Result), equal to one run() each.  Raises NdbError on
         the first failing problem's status after every other one has run."""
@@ -169,7 +178,7 @@ class Context:
             jobs[j].nn_out = nn.ctypes.data if nn is not None and nn.size else None
             jobs[j].cluster_index_out = ci.ctypes.data if ci.size else None
             outs.append((nn, ci))
-        flags = (lib.FLAG_FULL_COUNT if full_count else 0) | (lib.FLAG_APPROXIMATE if approximate else 0)
+        flags = _flags(full_count, approximate, exact_count, tensor_filter)
         st = self._lib.ndb_b200_run_batched(self._h, jobs, len(pts), flags)
         self.last_jobs = jobs
         lib.check(st, "ndb_b200_run_batched", self._h)

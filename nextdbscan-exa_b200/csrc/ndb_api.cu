@@ -13,6 +13,7 @@
 #include "../../include/ndb_b200.h"
 #include "ndb_internal.h"
 #include "ndb_kernels.cuh"
+#include "ndb_tc.cuh"
 
 using namespace ndb;
 
@@ -35,6 +36,8 @@ struct ndb_ctx {
     DevBuf nbr_list;
     size_t list_budget = size_t(8) << 30;  // largest list buffer the context may use (else: scan border)
     int list_cap = 0;                 // entries per point, 0 when the lists are off
+    bool tc_count = false;            // neighbour count on the tensor-core filter
+    int sm_count = 148;
     // scratch
     DevBuf sort_hist, scan_scratch, small;  // small: counters, bbox, scalars
     // batched runs: job table, per-job bounding boxes, cell -> job, per-job counters
@@ -71,6 +74,7 @@ namespace {
 constexpr size_t kSmallBboxOff = 0;          // int[2*kMaxDim]
 constexpr size_t kSmallInvalidOff = 256;     // u64
 constexpr size_t kSmallCountersOff = 512;    // u64[8]: 0 clusters 1 noise 2 count pairs 3 union pairs 4 border pairs
+                                             // 5 band pairs 6 work counter of the persistent count kernel
 constexpr size_t kSmallScalarOff = 1024;     // u32[8]: 0 n_cells 1 n_items 2 n_cores
 constexpr size_t kSmallErrOff = 1536;        // int
 constexpr size_t kSmallStencilOff = 2048;    // int4[kMaxRows]: stencil rows of the current job
@@ -343,6 +347,59 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
 }
 
 template <int D>
+void count_phase(ndb_ctx *ctx);
+
+// The tensor-core filter's preconditions: d at or above the threshold (8 unless
+// NDB_TC_MIN_DIM raises it), the eps grid (row tables of <= 32 rows), eps^2 a
+// normal float far from under- and overflow, and coordinates within +-2^60 so that
+// no centred difference or squared norm overflows.  Results never depend on it.
+inline bool tc_eligible(int d, float e2, const double *lo, const double *hi, bool linked, int n_rows,
+                        uint32_t flags) {
+    static const int min_dim = [] {
+        const char *s = getenv("NDB_TC_MIN_DIM");
+        const int v = s ? atoi(s) : tc::kMinDim;
+        return v < tc::kMinDim ? tc::kMinDim : v;
+    }();
+    if (d < min_dim || (flags & NDB_FLAG_EXACT_COUNT) || linked || n_rows > kWarp) return false;
+    if (!(e2 >= 0x1p-100f && e2 <= 0x1p100f)) return false;
+    for (int a = 0; a < d; ++a)
+        if (!(fabs(lo[a]) <= 0x1p60 && fabs(hi[a]) <= 0x1p60)) return false;
+    return true;
+}
+
+// Tile fill: the tensor kernel stages every candidate row once per item and its
+// epilogue cost per tile is mostly fixed, so it pays only when items are full
+// (many points per cell).  Measured on B200: at about 11 points per item the exact
+// kernel is faster at d = 8 and even at d = 16.  NDB_TC_MIN_FILL overrides the
+// threshold (points per item, default 24); NDB_FLAG_TENSOR_FILTER skips the test.
+inline bool tc_fill_ok(int64_t nv, int64_t n_items) {
+    static const double min_fill = [] {
+        const char *s = getenv("NDB_TC_MIN_FILL");
+        return s ? atof(s) : 24.0;
+    }();
+    return n_items > 0 && (double)nv >= min_fill * (double)n_items;
+}
+
+template <int D>
+void launch_count_tc(ndb_ctx *ctx, int64_t n_items, const int2 *items, const int32_t *cell_start, const int2 *nbr,
+                     int n_rows, const float *xs, float e2, int min_pts, bool early, int32_t *nn_sorted,
+                     int32_t *list, int list_cap, int list_stride, const JobDev *jobs, const int32_t *cell_job) {
+    if constexpr (D >= tc::kMinDim) {
+        cudaStream_t st = ctx->stream;
+        unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
+        unsigned int *work = reinterpret_cast<unsigned int *>(counters + 6);
+        ck(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
+        const unsigned grid = (unsigned)std::min<int64_t>(n_items, (int64_t)ctx->sm_count * 4);
+        ++launch_counter(), tc::count_tc_kernel<D><<<grid, tc::kThreads, 0, st>>>(
+            items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, early ? 1 : 0, nn_sorted, list, list_cap,
+            list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job);
+        ck(ctx, cudaGetLastError());
+    } else {
+        throw Fail{NDB_ERR_INVALID_ARGUMENT};
+    }
+}
+
+template <int D>
 void count_phase(ndb_ctx *ctx) {
     cudaStream_t st = ctx->stream;
     unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
@@ -358,7 +415,12 @@ void count_phase(ndb_ctx *ctx) {
     }
     int32_t *list = ctx->list_cap ? ctx->nbr_list.as<int32_t>() : nullptr;
     cudaEventRecord(ctx->kev[2], st);
-    if (ctx->n_items > 0) {
+    ctx->tc_count = ctx->tc_count && ((ctx->flags_run & NDB_FLAG_TENSOR_FILTER) || tc_fill_ok(ctx->nv, ctx->n_items));
+    if (ctx->n_items > 0 && ctx->tc_count) {
+        launch_count_tc<D>(ctx, ctx->n_items, ctx->items.as<int2>(), ctx->cell_start.as<int32_t>(),
+                           ctx->nbr.as<int2>(), ctx->n_rows, ctx->xs.as<float>(), ctx->e2, ctx->min_pts, early,
+                           ctx->nn_sorted.as<int32_t>(), list, ctx->list_cap, ctx->list_cap, nullptr, nullptr);
+    } else if (ctx->n_items > 0) {
         if (early)
             ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
@@ -577,6 +639,7 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->n_rows = pl.st.n_rows;
     ctx->cell_units = pl.cell_units ? 1 : 0;
     if (pl.st.n_rows > kWarp) return NDB_ERR_INVALID_ARGUMENT;  // row tables hold one row per lane
+    ctx->tc_count = tc_eligible(D, ctx->e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
 
     classify_dispatch<D>(ctx, pl);
 
@@ -605,6 +668,9 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->stats.same_cell_linked = ctx->cell_units;
     ctx->stats.key_bits = pl.key_bits;
     ctx->stats.count_pairs = (int64_t)h_counters[2];
+    ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
+    ctx->stats.band_pairs = (int64_t)h_counters[5];
+    ctx->stats.tensor_filter = ctx->tc_count ? 1 : 0;
     ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
     ctx->stats.ms_count = elapsed(ctx->ev[1], ctx->ev[2]);
     ctx->stats.ms_sort_kernels = elapsed(ctx->kev[0], ctx->kev[1]);
@@ -639,6 +705,8 @@ ndb_status labels_impl(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
     ctx->result.n = (int32_t)n;
     ctx->stats.union_pairs = (int64_t)h_counters[3];
     ctx->stats.border_pairs = (int64_t)h_counters[4];
+    ctx->stats.union_pair_dims = (int64_t)h_counters[3] * D;
+    ctx->stats.border_pair_dims = (int64_t)h_counters[4] * D;
     ctx->stats.ms_union = elapsed(ctx->ev[2], ctx->ev[3]);
     ctx->stats.ms_border = elapsed(ctx->ev[3], ctx->ev[4]);
     ctx->stats.ms_union_kernel = elapsed(ctx->kev[4], ctx->kev[5]);
@@ -706,6 +774,9 @@ ndb_status ndb_b200_create(ndb_ctx **out, int32_t device) {
     if (cudaSetDevice(device) != cudaSuccess) return NDB_ERR_NO_DEVICE;
     ndb_ctx *ctx = new ndb_ctx();
     ctx->device = device;
+    if (cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        ctx->sm_count <= 0)
+        ctx->sm_count = 148;
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return NDB_ERR_CUDA;
@@ -759,7 +830,8 @@ ndb_status ndb_b200_classify(ndb_ctx *ctx, const float *coords, int64_t n, int32
                              uint32_t flags, int32_t *nn_out) {
     ndb_status s = check_ctx(ctx);
     if (s != NDB_OK) return s;
-    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS)) return NDB_ERR_INVALID_ARGUMENT;
+    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS | NDB_FLAG_EXACT_COUNT |
+                  NDB_FLAG_TENSOR_FILTER)) return NDB_ERR_INVALID_ARGUMENT;
     if (n < 0) return NDB_ERR_INVALID_ARGUMENT;
     if (n > NDB_MAX_POINTS) return NDB_ERR_TOO_MANY_POINTS;
     if (d < 1 || d > NDB_MAX_DIM) return NDB_ERR_UNSUPPORTED_DIM;
@@ -873,6 +945,7 @@ struct BatchPlan {
     int key_bits = 0;
     int linked = 0;
     int list_stride = 0;
+    bool tc = false;  // neighbour count on the tensor-core filter (every job eligible)
     int64_t total_n = 0, nv = 0;
 };
 
@@ -890,6 +963,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     for (auto &j : bp.jd) max_n = std::max<int64_t>(max_n, j.n);
     const unsigned gx = (unsigned)std::min<int64_t>((max_n + kBlock - 1) / kBlock, 64);
 
+    cudaEventRecord(ctx->ev[0], st);
     // composite keys and the sort
     ensure(ctx, ctx->keys0, n * sizeof(K));
     ensure(ctx, ctx->keys1, n * sizeof(K));
@@ -903,6 +977,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         ctx->coords.as<float>(), jobs_dev, invalid_key, ctx->keys0.as<K>(), ctx->ids0.as<int32_t>());
     ck(ctx, cudaGetLastError());
     bool in_first = true;
+    cudaEventRecord(ctx->kev[0], st);
     if (sizeof(K) == 4)
         ck(ctx, radix_sort_pairs_u32(reinterpret_cast<uint32_t *>(ctx->keys0.ptr), ctx->ids0.as<int32_t>(),
                                      reinterpret_cast<uint32_t *>(ctx->keys1.ptr), ctx->ids1.as<int32_t>(), n,
@@ -913,6 +988,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
                                      reinterpret_cast<uint64_t *>(ctx->keys1.ptr), ctx->ids1.as<int32_t>(), n,
                                      bp.key_bits, ctx->sort_hist.as<uint32_t>(), ctx->scan_scratch.as<uint32_t>(),
                                      &in_first, st));
+    cudaEventRecord(ctx->kev[1], st);
     if (!in_first) {
         std::swap(ctx->keys0, ctx->keys1);
         std::swap(ctx->ids0, ctx->ids1);
@@ -986,7 +1062,14 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     }
     const unsigned grid = (unsigned)((n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
     const bool early = (flags & NDB_FLAG_FULL_COUNT) == 0;
-    if (n_items > 0) {
+    cudaEventRecord(ctx->ev[1], st);
+    cudaEventRecord(ctx->kev[2], st);
+    bp.tc = bp.tc && ((flags & NDB_FLAG_TENSOR_FILTER) || tc_fill_ok(nv, n_items));
+    if (n_items > 0 && bp.tc) {
+        launch_count_tc<D>(ctx, n_items, ctx->items.as<int2>(), ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(),
+                           n_rows, ctx->xs.as<float>(), 0.0f, 0, early, ctx->nn_sorted.as<int32_t>(), list, 0,
+                           bp.list_stride, jobs_dev, cell_job);
+    } else if (n_items > 0) {
         if (early)
             ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
@@ -999,6 +1082,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
                 jobs_dev, cell_job);
         ck(ctx, cudaGetLastError());
     }
+    cudaEventRecord(ctx->kev[3], st);
     const int64_t n_words = (n + 31) / 32;
     ensure(ctx, ctx->core_sorted, n + 1);
     ensure(ctx, ctx->cell_has_core, n_cells + 1);
@@ -1014,6 +1098,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     ck(ctx, cudaGetLastError());
     ck(ctx, scan_exclusive_u32(ctx->core_prefix.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), n_words, scal + 2,
                                ctx->scan_scratch.as<uint32_t>(), st));
+    cudaEventRecord(ctx->ev[2], st);
 
     // union-find, canonical ids, border points
     const int64_t n_units = bp.linked ? n_cells : nv;
@@ -1027,6 +1112,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     ++launch_counter(), iota_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units);
     ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units,
                                                                            kNoCluster);
+    cudaEventRecord(ctx->kev[4], st);
     if (n_items > 0) {
         if (bp.linked) {
             ++launch_counter(), union_near_kernel<D, K><<<blocks_for(n_cells), kBlock, 0, st>>>(
@@ -1047,6 +1133,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         }
         ck(ctx, cudaGetLastError());
     }
+    cudaEventRecord(ctx->kev[5], st);
     ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units, err);
     ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
         nv, ctx->core_sorted.as<uint8_t>(), perm, ctx->pcell.as<int32_t>(), bp.linked, ctx->core_bits.as<uint32_t>(),
@@ -1058,11 +1145,14 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         ++launch_counter(), cell_ids_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
             n_cells, ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>(),
             ctx->cell_cid.as<int32_t>(), counters, cell_job, jc);
+    cudaEventRecord(ctx->ev[3], st);
+    cudaEventRecord(ctx->kev[6], st);
     if (bp.list_stride > 0)
         ++launch_counter(), border_list_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
             nv, ctx->nn_sorted.as<int32_t>(), list, bp.list_stride, ctx->core_sorted.as<uint8_t>(), bp.linked,
             ctx->pcell.as<int32_t>(), ctx->cell_cid.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters + 4);
     ck(ctx, cudaGetLastError());
+    cudaEventRecord(ctx->kev[7], st);
 
     // outputs straight into each job's buffers, per-job meta
     ++launch_counter(), scatter_nn_kernel<<<blocks_for(n), kBlock, 0, st>>>(ctx->nn_sorted.as<int32_t>(), nv, n, perm,
@@ -1073,8 +1163,11 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     ++launch_counter(), job_cores_kernel<<<blocks_for(nj), kBlock, 0, st>>>(
         jobs_dev, nj, ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), n, jc);
     ck(ctx, cudaGetLastError());
+    cudaEventRecord(ctx->ev[4], st);
     std::vector<unsigned long long> h_jc((size_t)4 * nj);
+    unsigned long long h_pairs[4] = {0, 0, 0, 0};  // count, union, border, band pairs (running totals)
     int h_err = 0;
+    ck(ctx, cudaMemcpyAsync(h_pairs, counters + 2, sizeof(h_pairs), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_jc.data(), jc, (size_t)4 * nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             st));
     ck(ctx, cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1091,6 +1184,37 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         }
     }
     ck(ctx, cudaStreamSynchronize(st));
+    // statistics summed over the pipelines of one batched call
+    ndb_stats &S = ctx->stats;
+    S.pipelines += 1;
+    // pair counters run on over the pipelines of a call: this pipeline's share
+    const int64_t dc = (int64_t)h_pairs[0] - S.count_pairs, du = (int64_t)h_pairs[1] - S.union_pairs,
+                  db = (int64_t)h_pairs[2] - S.border_pairs;
+    S.band_pairs = (int64_t)h_pairs[3];
+    S.tensor_filter |= bp.tc ? 1 : 0;
+    S.count_pairs += dc;
+    S.union_pairs += du;
+    S.border_pairs += db;
+    S.count_pair_dims += dc * D;
+    S.union_pair_dims += du * D;
+    S.border_pair_dims += db * D;
+    S.n_valid += nv;
+    S.n_cells += n_cells;
+    S.n_tiles += n_items;
+    S.grid_dims = std::max(S.grid_dims, bp.jd[0].g.k);
+    S.stencil_rows = std::max(S.stencil_rows, n_rows);
+    S.same_cell_linked |= bp.linked;
+    S.key_bits = std::max(S.key_bits, bp.key_bits);
+    S.sort_passes += (bp.key_bits + 7) / 8;
+    S.key_bytes = std::max(S.key_bytes, (int32_t)sizeof(K));
+    S.ms_grid += elapsed(ctx->ev[0], ctx->ev[1]);
+    S.ms_count += elapsed(ctx->ev[1], ctx->ev[2]);
+    S.ms_union += elapsed(ctx->ev[2], ctx->ev[3]);
+    S.ms_border += elapsed(ctx->ev[3], ctx->ev[4]);
+    S.ms_sort_kernels += elapsed(ctx->kev[0], ctx->kev[1]);
+    S.ms_count_kernel += elapsed(ctx->kev[2], ctx->kev[3]);
+    S.ms_union_kernel += elapsed(ctx->kev[4], ctx->kev[5]);
+    S.ms_border_kernel += elapsed(ctx->kev[6], ctx->kev[7]);
     for (int m = 0; m < nj; ++m) {
         ndb_job &J = jobs[members[m]];
         J.result.clusters = (int32_t)h_jc[4 * m + 0];
@@ -1178,11 +1302,12 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
             hi[a] = jnv > 0 ? dec(h_lo_hi[(size_t)m * 2 * D + D + a]) : 0.0;
         }
         const Plan pl = plan_grid(D, jd.e2, lo, hi);
+        const bool job_tc = tc_eligible(D, jd.e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
         double cells = 1;
         for (int a = 0; a < pl.g.k; ++a) cells *= (double)pl.g.g[a];
         bool keep = (pl.cell_units ? 1 : 0) == bp.linked && jd.min_pts - 1 <= kMaxListCap &&
                     (double)key_base + cells < ldexp(1.0, 62);
-        if (keep && have_stencil) keep = pl.st.n_rows == bp.st.n_rows;
+        if (keep && have_stencil) keep = pl.st.n_rows == bp.st.n_rows && job_tc == bp.tc;  // one count kernel
         if (!keep) {
             solo.push_back(members[m]);
             continue;
@@ -1190,6 +1315,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
         kept.push_back(members[m]);
         if (!have_stencil) {
             bp.st = pl.st;
+            bp.tc = job_tc;
             have_stencil = true;
         }
         jd.g = pl.g;
@@ -1252,7 +1378,8 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     ndb_status s = check_ctx(ctx);
     if (s != NDB_OK) return s;
     if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return NDB_ERR_INVALID_ARGUMENT;
-    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS)) return NDB_ERR_INVALID_ARGUMENT;
+    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS | NDB_FLAG_EXACT_COUNT |
+                  NDB_FLAG_TENSOR_FILTER)) return NDB_ERR_INVALID_ARGUMENT;
     ctx->have_state = false;
     ctx->have_labels = false;
     ctx->stats = ndb_stats{};
@@ -1313,7 +1440,10 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
             if (gs != NDB_OK && first == NDB_OK) first = gs;
         }
     }
-    // jobs the pipeline could not take: one call each
+    // statistics of the pipelines, then of the jobs the pipelines could not take,
+    // which run one call each
+    ndb_stats acc = ctx->stats;
+    acc.kernel_launches = launch_counter();
     for (int i : solo) {
         ndb_job &J = jobs[i];
         ndb_result r{};
@@ -1322,7 +1452,31 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
         J.status = js;
         if (js == NDB_OK) J.result = r;
         else if (first == NDB_OK) first = js;
+        const ndb_stats &s1 = ctx->stats;
+        acc.n_valid += s1.n_valid;
+        acc.n_cells += s1.n_cells;
+        acc.n_tiles += s1.n_tiles;
+        acc.count_pairs += s1.count_pairs;
+        acc.union_pairs += s1.union_pairs;
+        acc.border_pairs += s1.border_pairs;
+        acc.band_pairs += s1.band_pairs;
+        acc.tensor_filter |= s1.tensor_filter;
+        acc.count_pair_dims += s1.count_pair_dims;
+        acc.union_pair_dims += s1.union_pair_dims;
+        acc.border_pair_dims += s1.border_pair_dims;
+        acc.ms_grid += s1.ms_grid;
+        acc.ms_count += s1.ms_count;
+        acc.ms_union += s1.ms_union;
+        acc.ms_border += s1.ms_border;
+        acc.ms_sort_kernels += s1.ms_sort_kernels;
+        acc.ms_count_kernel += s1.ms_count_kernel;
+        acc.ms_union_kernel += s1.ms_union_kernel;
+        acc.ms_border_kernel += s1.ms_border_kernel;
+        acc.sort_passes += s1.sort_passes;
+        acc.kernel_launches += s1.kernel_launches;
     }
+    acc.solo_jobs = (int32_t)solo.size();
+    ctx->stats = acc;
     ctx->have_state = false;
     ctx->have_labels = false;
     return first;

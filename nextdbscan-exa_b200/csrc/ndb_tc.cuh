@@ -1,0 +1,416 @@
+// ndb_tc.cuh -- tensor-core filtered neighbour count for d >= 8 (sm_100a).
+//
+// The exact predicate (data_process.cpp:443-447) costs 3d separately rounded FP32
+// operations per pair.  For d >= 8 the count runs instead on Gram tiles from the
+// 5th-generation tensor cores: for an item (up to 32 points i of one cell) and a
+// tile of 128 candidates j, one CTA computes
+//
+//     D~(i,j) = |a_i|^2 + |b_j|^2 - 2 a_i.b_j,   a = x_i - o, b = x_j - o,
+//
+// with o the item's first point, a.b from three TF32 products (hi.hi + hi.lo +
+// lo.hi of the split a = hi + lo) accumulated in FP32 in tensor memory.  A pair is
+// a hit when D~ is below eps^2 by more than a rigorous bound on the filter's error,
+// a miss when above by more than it, and otherwise (the guard band) it is rechecked
+// with the reference's own FP32 arithmetic.  Counts, core flags and neighbour lists
+// are therefore identical to the exact kernel's.
+//
+// Error bound (per pair, u = 2^-24, t = 2^-11 the TF32 rounding unit, K the padded
+// dimension):  |D~ - |x_i - x_j|^2| <= kappa (n_i + n_j) with n = |a|^2, from
+//   the split (3 t^2 |a||b|), the FP32 accumulation of 3K exact TF32 products
+//   (assumed no worse than 4u per addition of the running magnitude), the FP32
+//   norms (K u n), the centring x - o (4u (n_i + n_j)) and the rounding of the
+//   comparison value; kappa = (10 + 8K) 2^-22 is about twice their sum.
+// The reference's FP32 sum itself differs from the exact distance by at most
+// (d + 2) u relatively; gamma = 2 (K + 8) u covers it.
+#pragma once
+#include "ndb_kernels.cuh"
+
+namespace ndb {
+namespace tc {
+
+constexpr int kM = 128;              // candidates per tile: MMA M, TMEM lanes
+constexpr int kN = 32;               // points of one item: MMA N, TMEM columns per buffer
+constexpr int kThreads = 128;        // four warps, one per TMEM lane quadrant
+constexpr uint32_t kTmemCols = 64;   // two accumulator buffers
+constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kMinDim = 8;           // default: the tensor filter runs for d >= 8
+
+template <int D>
+struct KPad {
+    static constexpr int v = D <= 8 ? 8 : 16;
+};
+
+template <int KP>
+__host__ __device__ constexpr float kappa() {
+    return (10.0f + 8.0f * KP) * (1.0f / 4194304.0f);  // 2^-22
+}
+template <int KP>
+__host__ __device__ constexpr float gamma_rel() {
+    return 2.0f * (KP + 8) * (1.0f / 16777216.0f);  // 2^-24
+}
+constexpr float kSigma = 8.0f / 16777216.0f;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: 8-row core matrices of
+// 16-byte rows, the next 16-byte K chunk lbo bytes away, the next 8 rows sbo bytes
+// away; bits 46-47 = 1 (the sm_100 descriptor version).
+__device__ __forceinline__ uint64_t desc_kmajor(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::tf32: FP32 accumulator (bits 4-5 = 1), A and B
+// TF32 (bits 7-9, 10-12 = 2), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kN >> 3) << 17) |
+                            ((uint32_t)(kM >> 4) << 24);
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase of the given parity; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+// 32 consecutive accumulator columns of this thread's TMEM lane.  The load and
+// its wait are one asm statement: the destination registers are undefined until
+// tcgen05.wait::ld, so no use of them may be scheduled in between.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+}
+
+// 32x32 bit-matrix transpose across a warp: lane l holds row l (bit c = column
+// c) on entry and column l (bit r = row r) on return.
+__device__ __forceinline__ unsigned transpose32(unsigned x, int lane) {
+    const unsigned masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        const int j = 16 >> s;
+        const unsigned m = masks[s];
+        const unsigned y = __shfl_xor_sync(kFull, x, j);
+        x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
+    }
+    return x;
+}
+
+// Operand tile in shared memory: element (row r, k) of an R-row tile at
+// ((k / 4) * R + r) * 16 + (k % 4) * 4 bytes (LBO = 16 R, SBO = 128).
+template <int KP>
+__device__ __forceinline__ void store_row(uint32_t *tile, int rows, int r, const uint32_t (&v)[KP]) {
+#pragma unroll
+    for (int q = 0; q < KP / 4; ++q)
+        *reinterpret_cast<uint4 *>(tile + ((size_t)q * rows + r) * 4) =
+            make_uint4(v[4 * q + 0], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// x - o, split into TF32 hi + lo, and |x - o|^2 (FP32)
+template <int D, int KP>
+__device__ __forceinline__ float centre_split(const float (&x)[D], const float (&o)[D], uint32_t (&hi)[KP],
+                                              uint32_t (&lo)[KP]) {
+    float n = 0.0f;
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+        const float a = k < D ? __fsub_rn(x[k], o[k]) : 0.0f;
+        hi[k] = tf32_rna(a);
+        lo[k] = tf32_rna(__fsub_rn(a, __uint_as_float(hi[k])));
+        n = __fmaf_rn(a, a, n);
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------------------
+// The count kernel.  Persistent CTAs take items from a work counter.  Per item:
+// warp 0 gathers the stencil rows, warp 1 stages the item's points (the MMA's B
+// operand, N = 32); then candidate tiles of 128 are staged by all threads (one
+// row each: load, centre, split, store) while the tensor core runs the previous
+// tile's three MMAs per K step into the other TMEM buffer.  Each thread owns one
+// TMEM lane = one candidate; it classifies its 32 columns, rechecks band pairs
+// exactly, and a warp transpose turns the row masks into per-column hit masks.
+// EARLY: columns leave the active set once their count reaches min_pts.
+// Neighbour lists: the first list_cap hits of each column (complete for every
+// point that stays below min_pts), slots reserved by shared-memory atomics.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
+    const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
+    const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts, int early,
+    int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
+    unsigned long long *__restrict__ pair_counter, unsigned long long *__restrict__ band_counter,
+    unsigned int *__restrict__ work, int *__restrict__ err, const JobDev *__restrict__ jobs,
+    const int32_t *__restrict__ cell_job) {
+    constexpr int KP = KPad<D>::v, P = Stride<D>::P, KC = KP / 4;
+    __shared__ __align__(1024) uint32_t s_a[2][2][KC * kM * 4];  // [buffer][hi, lo] candidate tiles
+    __shared__ __align__(128) uint32_t s_b[2][KC * kN * 4];      // [hi, lo] the item's points
+    __shared__ __align__(16) float s_x[kN * P];                   // the item's points as stored
+    __shared__ __align__(16) float s_ni[kN];
+    __shared__ int s_j[2][kM];
+    __shared__ int s_part[2][4][kN];
+    __shared__ int s_listn[kN];
+    __shared__ RowTable s_rt;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_item, s_abort;
+    __shared__ float s_nmax;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (warp == 0) {
+        tmem_alloc(&s_tmem, kTmemCols);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = s_tmem;
+    uint32_t phase = 0, pending = 0;  // per buffer: parity of its next completion; MMAs not yet waited for
+    unsigned long long pairs = 0, band = 0;
+    const float kap = kappa<KP>();
+
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(work, 1u);
+        __syncthreads();
+        const int64_t item_id = s_item;
+        if (item_id >= n_items || s_abort) break;
+        const int2 item = items[item_id];
+        const int cell = item.x, p0 = item.y;
+        const int cnt = min(kN, cell_start[cell + 1] - p0);
+        float e2j = e2;
+        int mp = min_pts, lc = list_cap;
+        if (jobs) {
+            const JobDev &J = jobs[cell_job[cell]];
+            e2j = J.e2;
+            mp = J.min_pts;
+            lc = J.list_cap;
+        }
+        float o[D];
+        load_point<D>(xs, p0, o);
+        if (warp == 0) {
+            gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, s_rt, lane);
+            s_listn[lane] = 0;
+        } else if (warp == 1) {
+            float x[D];
+            load_point<D>(xs, p0 + min(lane, cnt - 1), x);
+            store_point_smem<D>(s_x + lane * P, x);
+            uint32_t hi[KP], lo[KP];
+            const float n = centre_split<D, KP>(x, o, hi, lo);
+            store_row<KP>(s_b[0], kN, lane, hi);
+            store_row<KP>(s_b[1], kN, lane, lo);
+            s_ni[lane] = n;
+            float nm = lane < cnt ? n : 0.0f;
+#pragma unroll
+            for (int s = 16; s > 0; s >>= 1) nm = fmaxf(nm, __shfl_xor_sync(kFull, nm, s));
+            if (lane == 0) s_nmax = nm;
+            fence_async_smem();
+        }
+        __syncthreads();
+        const int total = s_rt.off[n_rows];
+        const float nmax = s_nmax;
+        const float e2lo = e2j * (1.0f - gamma_rel<KP>()), e2hi = e2j * (1.0f + gamma_rel<KP>());
+        const int n_tiles = (total + kM - 1) / kM;
+        unsigned act = cnt >= kN ? kFull : ((1u << cnt) - 1u);
+        int run = 0, totals = 0;  // lane c: this warp's hits of column c; all warps' hits after the last tile
+
+        // One candidate row per thread.  fetch: the row's point index (a cursor over
+        // the stencil rows, advanced as the tile index grows) and its coordinates,
+        // loaded into registers before the previous tile is processed so that the
+        // load latency hides behind that work.  stage: centre, split, store, and the
+        // thresholds of the comparison value v = n_i - 2 g (hit if v <= tlo, miss if
+        // v > thi).
+        int row = 0;
+        auto fetch = [&](int t, int &jrow, float (&x)[D]) {
+            const int v = t * kM + tid;
+            jrow = -1;
+            if (v < total) {
+                while (s_rt.off[row + 1] <= v) ++row;
+                jrow = s_rt.start[row] + (v - s_rt.off[row]);
+                load_point<D>(xs, jrow, x);
+            }
+        };
+        auto stage = [&](int buf, int jrow, const float (&x)[D], float &tlo, float &thi) {
+            uint32_t hi[KP], lo[KP];
+            float n = 0.0f;
+            if (jrow >= 0) {
+                n = centre_split<D, KP>(x, o, hi, lo);
+            } else {
+#pragma unroll
+                for (int k = 0; k < KP; ++k) hi[k] = lo[k] = 0u;
+            }
+            store_row<KP>(s_a[buf][0], kM, tid, hi);
+            store_row<KP>(s_a[buf][1], kM, tid, lo);
+            s_j[buf][tid] = jrow;
+            const float slack = __fadd_rn(__fmul_rn(kap, __fadd_rn(nmax, n)), __fmul_rn(kSigma, e2j));
+            tlo = jrow >= 0 ? __fsub_rn(__fsub_rn(e2lo, n), slack) : -INFINITY;
+            thi = jrow >= 0 ? __fadd_rn(__fsub_rn(e2hi, n), slack) : -INFINITY;
+        };
+        auto issue = [&](int t) {
+            const int b = t & 1;
+            const uint32_t d = tmem + (uint32_t)(b * kN);
+            const uint32_t ah = smem_u32(s_a[b][0]), al = smem_u32(s_a[b][1]);
+            const uint32_t bh = smem_u32(s_b[0]), bl = smem_u32(s_b[1]);
+#pragma unroll
+            for (int s = 0; s < KP / 8; ++s) {
+                const uint32_t ao = (uint32_t)(s * 2 * kM * 16), bo = (uint32_t)(s * 2 * kN * 16);
+                const uint64_t dah = desc_kmajor(ah + ao, kM * 16, 128), dal = desc_kmajor(al + ao, kM * 16, 128);
+                const uint64_t dbh = desc_kmajor(bh + bo, kN * 16, 128), dbl = desc_kmajor(bl + bo, kN * 16, 128);
+                mma_tf32(d, dah, dbh, s > 0 ? 1u : 0u);
+                mma_tf32(d, dah, dbl, 1u);
+                mma_tf32(d, dal, dbh, 1u);
+            }
+            mma_commit(&s_bar[b]);
+        };
+
+        int j_cur = -1, j_nxt = -1;
+        float tlo_cur = -INFINITY, thi_cur = -INFINITY, tlo_nxt = -INFINITY, thi_nxt = -INFINITY;
+        float x_nxt[D];
+        fetch(0, j_cur, x_nxt);
+        stage(0, j_cur, x_nxt, tlo_cur, thi_cur);
+        fence_async_smem();
+        tc_before_sync();
+        __syncthreads();
+        tc_after_sync();
+        if (tid == 0) issue(0);
+        pending |= 1u;
+        for (int t = 1; t <= n_tiles; ++t) {
+            const int pb = (t - 1) & 1;
+            if (t < n_tiles) fetch(t, j_nxt, x_nxt);
+            const bool ok = mbar_wait(&s_bar[pb], (phase >> pb) & 1u);
+            if (ok) {
+                phase ^= 1u << pb;
+                pending &= ~(1u << pb);
+                tc_after_sync();
+                uint32_t g[32];
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(pb * kN), g);
+                unsigned hb = 0, bb = 0;
+#pragma unroll
+                for (int c = 0; c < kN; ++c) {
+                    if ((act >> c) & 1u) {
+                        const float v = __fmaf_rn(-2.0f, __uint_as_float(g[c]), s_ni[c]);
+                        hb |= (v <= tlo_cur ? 1u : 0u) << c;
+                        bb |= (v <= thi_cur ? 1u : 0u) << c;
+                    }
+                }
+                bb &= ~hb;
+                if (__any_sync(kFull, bb != 0)) {
+                    if (bb) {
+                        float xj[D];
+                        load_point<D>(xs, j_cur, xj);
+                        band += (unsigned long long)__popc(bb);
+                        for (unsigned m = bb; m; m &= m - 1) {
+                            const int c = __ffs(m) - 1;
+                            float xi[D];
+                            load_point_smem<D>(s_x + c * P, xi);
+                            if (in_range<D>(xi, xj, e2j)) hb |= 1u << c;
+                        }
+                    }
+                }
+                const unsigned cm = transpose32(hb, lane);  // rows of this warp that hit column `lane`
+                if ((act >> lane) & 1u) {
+                    const int h = __popc(cm);
+                    run += h;
+                    if (nbr_list && h && totals < lc) {
+                        int slot = atomicAdd(&s_listn[lane], h);
+                        for (unsigned m = cm; m && slot < lc; m &= m - 1, ++slot)
+                            nbr_list[(int64_t)(p0 + lane) * list_stride + slot] = s_j[pb][warp * 32 + __ffs(m) - 1];
+                    }
+                }
+                s_part[t & 1][warp][lane] = run;
+                if (tid == 0) pairs += (unsigned long long)__popc(act) * (unsigned long long)min(kM, total - (t - 1) * kM);
+            } else {
+                s_abort = 1;
+                atomicExch(err, 2);
+            }
+            if (t < n_tiles) stage(t & 1, j_nxt, x_nxt, tlo_nxt, thi_nxt);
+            fence_async_smem();
+            tc_before_sync();
+            __syncthreads();
+            tc_after_sync();
+            if (s_abort) break;
+            totals = s_part[t & 1][0][lane] + s_part[t & 1][1][lane] + s_part[t & 1][2][lane] + s_part[t & 1][3][lane];
+            if (early) act = __ballot_sync(kFull, lane < cnt && totals < mp);
+            if (early && !act) break;
+            if (t < n_tiles) {
+                if (tid == 0) issue(t);
+                pending |= 1u << (t & 1);
+                j_cur = j_nxt;
+                tlo_cur = tlo_nxt;
+                thi_cur = thi_nxt;
+            }
+        }
+        if (s_abort) break;
+        if (warp == 0 && lane < cnt) nn_sorted[p0 + lane] = totals;
+    }
+    // MMAs still in flight after an abort: wait for them (bounded) before freeing TMEM
+    for (int b = 0; b < 2; ++b)
+        if ((pending >> b) & 1u) mbar_wait(&s_bar[b], (phase >> b) & 1u);
+    tc_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_after_sync();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+    if (tid == 0 && pairs) atomicAdd(pair_counter, pairs);
+    if (band) atomicAdd(band_counter, band);
+}
+
+}  // namespace tc
+}  // namespace ndb

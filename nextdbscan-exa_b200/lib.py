@@ -18,6 +18,8 @@ NDB_MAX_DIM = 16
 FLAG_APPROXIMATE = 0x1
 FLAG_FULL_COUNT = 0x2
 FLAG_DEVICE_PTRS = 0x4
+FLAG_EXACT_COUNT = 0x8
+FLAG_TENSOR_FILTER = 0x10
 
 STATUS = {
     0: "NDB_OK",
@@ -88,6 +90,13 @@ class NdbStats(ctypes.Structure):
         ("sort_passes", ctypes.c_int32),
         ("key_bytes", ctypes.c_int32),
         ("kernel_launches", ctypes.c_int32),
+        ("pipelines", ctypes.c_int32),
+        ("count_pair_dims", ctypes.c_int64),
+        ("union_pair_dims", ctypes.c_int64),
+        ("border_pair_dims", ctypes.c_int64),
+        ("solo_jobs", ctypes.c_int32),
+        ("tensor_filter", ctypes.c_int32),
+        ("band_pairs", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:
