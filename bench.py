@@ -325,7 +325,7 @@ def run_ours(args):
             fs = ctx.stats()
             fv = n * len(f_ms) / (sum(f_ms) / 1000.0)
             forms[name] = {"value": fv, "unit": UNIT, "ms_per_step": sum(f_ms) / len(f_ms),
-                           "count_kernel_ms": fs["ms_count_kernel"], "tensor_filter": bool(fs["tensor_filter"]),
+                           "count_kernel_ms": fs["ms_count_kernel"], "tensor_items": fs["tensor_items"],
                            "band_pairs": fs["band_pairs"], "filtered_pairs": fs["count_pairs"],
                            "identical_cluster_ids": bool(np.array_equal(ci.cpu().numpy(), ci_chosen))}
         forms["chosen_over_plain"] = value / world / forms["exact_fp32_count"]["value"]
@@ -387,8 +387,8 @@ def run_ours(args):
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk_sum,
             "gpu_launches": launches * args.steps, "count_forms": forms or None,
-            "tensor_filter": {"used": bool(s0["tensor_filter"]), "band_pairs": s0["band_pairs"],
-                              "filtered_pairs": s0["count_pairs"]},
+            "tensor_filter": {"used": bool(s0["tensor_filter"]), "items": s0["tensor_items"], "of_items": s0["n_tiles"],
+                              "band_pairs": s0["band_pairs"]},
             "result": {"clusters": res.clusters, "noise": res.noise, "core_count": res.core_count},
             "phases_ms": {k: round(statistics.mean(s[k] for s in stats), 4)
                           for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
@@ -578,6 +578,8 @@ def run_ours_batch(args):
                           for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
             "kernels_ms": {k: round(v, 4) for k, v in kern.items()},
             "pipelines": s0["pipelines"], "solo_jobs": s0["solo_jobs"],
+            "tensor_filter": {"used": bool(s0["tensor_filter"]), "items": s0["tensor_items"], "of_items": s0["n_tiles"],
+                              "band_pairs": s0["band_pairs"]},
             "pairs": {"count": s0["count_pairs"], "union": s0["union_pairs"], "border": s0["border_pairs"]},
         }
         print(json.dumps(line), flush=True)

@@ -115,6 +115,7 @@ typedef struct ndb_stats {
     int32_t solo_jobs;        /* batched runs: jobs the pipelines could not take, run one call each */
     int32_t tensor_filter;    /* 1 when the neighbour count ran on the tensor-core filter (d >= 8) */
     int64_t band_pairs;       /* pairs inside the filter's guard band, rechecked with the exact predicate */
+    int64_t tensor_items;     /* items (points of one cell, up to 32) counted on the tensor-core filter */
 } ndb_stats;
 
 typedef struct ndb_ctx ndb_ctx;

@@ -42,6 +42,8 @@ struct ndb_ctx {
     DevBuf sort_hist, scan_scratch, small;  // small: counters, bbox, scalars
     // batched runs: job table, per-job bounding boxes, cell -> job, per-job counters
     DevBuf jobs_dev, batch_bbox, cell_job, job_counters;
+    // items split between the tensor-core count (full items) and the exact one
+    DevBuf items_split;
 
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     // kernel-level events: sort, count, union, border (begin, end)
@@ -367,23 +369,26 @@ inline bool tc_eligible(int d, float e2, const double *lo, const double *hi, boo
     return true;
 }
 
-// Tile fill: the tensor kernel stages every candidate row once per item and its
-// epilogue cost per tile is mostly fixed, so it pays only when items are full
-// (many points per cell).  Measured on B200: at about 11 points per item the exact
-// kernel is faster at d = 8 and even at d = 16.  NDB_TC_MIN_FILL overrides the
-// threshold (points per item, default 24); NDB_FLAG_TENSOR_FILTER skips the test.
-inline bool tc_fill_ok(int64_t nv, int64_t n_items) {
-    static const double min_fill = [] {
-        const char *s = getenv("NDB_TC_MIN_FILL");
-        return s ? atof(s) : 24.0;
+// Which items the tensor kernel takes: it stages every candidate row once per item
+// and most of its per-tile epilogue is fixed, so it pays only for full items (many
+// points of one cell).  Measured on B200: with about 11 points per item the exact
+// kernel is faster even at d = 16.  Items with at least this many points go to the
+// tensor-core count, the rest to the exact kernel (NDB_TC_MIN_ITEM overrides it;
+// NDB_FLAG_TENSOR_FILTER sends every item).
+inline int tc_min_item() {
+    static const int v = [] {
+        const char *s = getenv("NDB_TC_MIN_ITEM");
+        const int x = s ? atoi(s) : 16;
+        return x < 1 ? 1 : x;
     }();
-    return n_items > 0 && (double)nv >= min_fill * (double)n_items;
+    return v;
 }
 
 template <int D>
 void launch_count_tc(ndb_ctx *ctx, int64_t n_items, const int2 *items, const int32_t *cell_start, const int2 *nbr,
                      int n_rows, const float *xs, float e2, int min_pts, bool early, int32_t *nn_sorted,
-                     int32_t *list, int list_cap, int list_stride, const JobDev *jobs, const int32_t *cell_job) {
+                     int32_t *list, int list_cap, int list_stride, const JobDev *jobs, const int32_t *cell_job,
+                     const uint32_t *n_items_dev) {
     if constexpr (D >= tc::kMinDim) {
         cudaStream_t st = ctx->stream;
         unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
@@ -392,11 +397,51 @@ void launch_count_tc(ndb_ctx *ctx, int64_t n_items, const int2 *items, const int
         const unsigned grid = (unsigned)std::min<int64_t>(n_items, (int64_t)ctx->sm_count * 4);
         ++launch_counter(), tc::count_tc_kernel<D><<<grid, tc::kThreads, 0, st>>>(
             items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, early ? 1 : 0, nn_sorted, list, list_cap,
-            list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job);
+            list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job,
+            n_items_dev);
         ck(ctx, cudaGetLastError());
     } else {
         throw Fail{NDB_ERR_INVALID_ARGUMENT};
     }
+}
+
+// The neighbour count of one pipeline.  tc: the tensor-core filter may run (input
+// eligible); then the items are split by size and each list goes to its kernel,
+// both launched at the upper bound and reading their list length on the device.
+template <int D>
+void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_items, const int2 *items,
+                 const int32_t *cell_start, const int2 *nbr, int n_rows, const float *xs, float e2, int min_pts,
+                 int dense_skip, int32_t *nn_sorted, int32_t *list, int list_cap, int list_stride,
+                 const JobDev *jobs, const int32_t *cell_job) {
+    if (n_items <= 0) return;
+    cudaStream_t st = ctx->stream;
+    unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
+    const int2 *ex_items = items;
+    const uint32_t *ex_n = nullptr;
+    if (tc) {
+        uint32_t *scal = small_at<uint32_t>(ctx, kSmallScalarOff);
+        ensure(ctx, ctx->items_split, (size_t)(2 * n_items + 2) * sizeof(int2));
+        int2 *tc_items = ctx->items_split.as<int2>();
+        int2 *rest = tc_items + n_items + 1;
+        ck(ctx, cudaMemsetAsync(scal + 4, 0, 2 * sizeof(uint32_t), st));
+        ++launch_counter(), split_items_kernel<<<blocks_for(n_items), kBlock, 0, st>>>(
+            items, n_items, cell_start, force_tc ? 1 : tc_min_item(), tc_items, scal + 4, rest, scal + 5);
+        ck(ctx, cudaGetLastError());
+        launch_count_tc<D>(ctx, n_items, tc_items, cell_start, nbr, n_rows, xs, e2, min_pts, early, nn_sorted, list,
+                           list_cap, list_stride, jobs, cell_job, scal + 4);
+        ex_items = rest;
+        ex_n = scal + 5;
+    }
+    const unsigned grid = (unsigned)((n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    if (early)
+        ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
+            ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
+            list_stride, counters + 2, jobs, cell_job, ex_n);
+    else
+        ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
+            ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
+            list_stride, counters + 2, jobs, cell_job, ex_n);
+    ck(ctx, cudaGetLastError());
 }
 
 template <int D>
@@ -415,24 +460,10 @@ void count_phase(ndb_ctx *ctx) {
     }
     int32_t *list = ctx->list_cap ? ctx->nbr_list.as<int32_t>() : nullptr;
     cudaEventRecord(ctx->kev[2], st);
-    ctx->tc_count = ctx->tc_count && ((ctx->flags_run & NDB_FLAG_TENSOR_FILTER) || tc_fill_ok(ctx->nv, ctx->n_items));
-    if (ctx->n_items > 0 && ctx->tc_count) {
-        launch_count_tc<D>(ctx, ctx->n_items, ctx->items.as<int2>(), ctx->cell_start.as<int32_t>(),
-                           ctx->nbr.as<int2>(), ctx->n_rows, ctx->xs.as<float>(), ctx->e2, ctx->min_pts, early,
-                           ctx->nn_sorted.as<int32_t>(), list, ctx->list_cap, ctx->list_cap, nullptr, nullptr);
-    } else if (ctx->n_items > 0) {
-        if (early)
-            ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
-                ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
-                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
-                ctx->list_cap, ctx->list_cap, counters + 2, nullptr, nullptr);
-        else
-            ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
-                ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
-                ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
-                ctx->list_cap, ctx->list_cap, counters + 2, nullptr, nullptr);
-        ck(ctx, cudaGetLastError());
-    }
+    count_items<D>(ctx, ctx->tc_count, (ctx->flags_run & NDB_FLAG_TENSOR_FILTER) != 0, early, ctx->n_items,
+                   ctx->items.as<int2>(), ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
+                   ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
+                   ctx->list_cap, ctx->list_cap, nullptr, nullptr);
     cudaEventRecord(ctx->kev[3], st);
 }
 
@@ -517,11 +548,22 @@ void labels_phase(ndb_ctx *ctx) {
                 ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
                 counters + 3, err, nullptr, nullptr);
         }
-        else
+        else {
+            if (ctx->list_cap > 0) {
+                ++launch_counter(), union_lists_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+                    nv, ctx->nn_sorted.as<int32_t>(), ctx->nbr_list.as<int32_t>(), ctx->list_cap, ctx->list_cap,
+                    ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(), err, nullptr, nullptr, nullptr);
+                ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
+                                                                                          n_units, err);
+            }
+            ++launch_counter(), cell_root_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
+                n_cells, ctx->cell_start.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+                ctx->parent.as<int32_t>(), ctx->cell_cid.as<int32_t>());
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                 ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
+                ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr, ctx->cell_cid.as<int32_t>());
+        }
         ck(ctx, cudaGetLastError());
     }
     cudaEventRecord(ctx->kev[5], st);
@@ -657,9 +699,13 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
             ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     }
     unsigned long long h_counters[8];
+    uint32_t h_tc_items = 0;
     ck(ctx, cudaMemcpyAsync(h_counters, small_at<unsigned long long>(ctx, kSmallCountersOff), sizeof(h_counters),
                             cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaMemcpyAsync(&h_tc_items, small_at<uint32_t>(ctx, kSmallScalarOff) + 4, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaStreamSynchronize(st));
+    ctx->stats.tensor_items = ctx->tc_count ? h_tc_items : 0;
     ctx->stats.n_valid = ctx->nv;
     ctx->stats.n_cells = ctx->n_cells;
     ctx->stats.n_tiles = ctx->n_items;
@@ -809,7 +855,7 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
                       &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
                       &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small,
                       &ctx->hash_keys,   &ctx->hash_vals, &ctx->nbr_list, &ctx->jobs_dev,
-                      &ctx->batch_bbox,  &ctx->cell_job,  &ctx->job_counters};
+                      &ctx->batch_bbox,  &ctx->cell_job,  &ctx->job_counters, &ctx->items_split};
     for (DevBuf *b : bufs) b->release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -1064,24 +1110,9 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     const bool early = (flags & NDB_FLAG_FULL_COUNT) == 0;
     cudaEventRecord(ctx->ev[1], st);
     cudaEventRecord(ctx->kev[2], st);
-    bp.tc = bp.tc && ((flags & NDB_FLAG_TENSOR_FILTER) || tc_fill_ok(nv, n_items));
-    if (n_items > 0 && bp.tc) {
-        launch_count_tc<D>(ctx, n_items, ctx->items.as<int2>(), ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(),
-                           n_rows, ctx->xs.as<float>(), 0.0f, 0, early, ctx->nn_sorted.as<int32_t>(), list, 0,
-                           bp.list_stride, jobs_dev, cell_job);
-    } else if (n_items > 0) {
-        if (early)
-            ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
-                ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
-                ctx->xs.as<float>(), 0.0f, 0, 0, ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, counters + 2,
-                jobs_dev, cell_job);
-        else
-            ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
-                ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
-                ctx->xs.as<float>(), 0.0f, 0, 0, ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, counters + 2,
-                jobs_dev, cell_job);
-        ck(ctx, cudaGetLastError());
-    }
+    count_items<D>(ctx, bp.tc, (flags & NDB_FLAG_TENSOR_FILTER) != 0, early, n_items, ctx->items.as<int2>(),
+                   ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows, ctx->xs.as<float>(), 0.0f, 0, 0,
+                   ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, jobs_dev, cell_job);
     cudaEventRecord(ctx->kev[3], st);
     const int64_t n_words = (n + 31) / 32;
     ensure(ctx, ctx->core_sorted, n + 1);
@@ -1126,10 +1157,20 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
                 ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
                 counters + 3, err, jobs_dev, cell_job);
         } else {
+            if (bp.list_stride > 0) {
+                ++launch_counter(), union_lists_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+                    nv, ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, ctx->core_sorted.as<uint8_t>(),
+                    ctx->parent.as<int32_t>(), err, jobs_dev, cell_job, ctx->pcell.as<int32_t>());
+                ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
+                                                                                          n_units, err);
+            }
+            ++launch_counter(), cell_root_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
+                n_cells, ctx->cell_start.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+                ctx->parent.as<int32_t>(), ctx->cell_cid.as<int32_t>());
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
                 ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                ctx->parent.as<int32_t>(), counters + 3, err, jobs_dev, cell_job);
+                ctx->parent.as<int32_t>(), counters + 3, err, jobs_dev, cell_job, ctx->cell_cid.as<int32_t>());
         }
         ck(ctx, cudaGetLastError());
     }
@@ -1166,7 +1207,10 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     cudaEventRecord(ctx->ev[4], st);
     std::vector<unsigned long long> h_jc((size_t)4 * nj);
     unsigned long long h_pairs[4] = {0, 0, 0, 0};  // count, union, border, band pairs (running totals)
+    uint32_t h_tc_items = 0;
     int h_err = 0;
+    if (bp.tc)
+        ck(ctx, cudaMemcpyAsync(&h_tc_items, scal + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_pairs, counters + 2, sizeof(h_pairs), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_jc.data(), jc, (size_t)4 * nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             st));
@@ -1191,6 +1235,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     const int64_t dc = (int64_t)h_pairs[0] - S.count_pairs, du = (int64_t)h_pairs[1] - S.union_pairs,
                   db = (int64_t)h_pairs[2] - S.border_pairs;
     S.band_pairs = (int64_t)h_pairs[3];
+    S.tensor_items += h_tc_items;
     S.tensor_filter |= bp.tc ? 1 : 0;
     S.count_pairs += dc;
     S.union_pairs += du;
@@ -1460,6 +1505,7 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
         acc.union_pairs += s1.union_pairs;
         acc.border_pairs += s1.border_pairs;
         acc.band_pairs += s1.band_pairs;
+        acc.tensor_items += s1.tensor_items;
         acc.tensor_filter |= s1.tensor_filter;
         acc.count_pair_dims += s1.count_pair_dims;
         acc.union_pair_dims += s1.union_pair_dims;

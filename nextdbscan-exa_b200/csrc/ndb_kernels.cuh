@@ -395,6 +395,35 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
     }
 }
 
+// Items into two lists: those with at least min_cnt points (full tiles: the
+// tensor-core count) and the rest (the exact kernel).  Order within a list is
+// free; both counts land in device memory.
+__global__ void split_items_kernel(const int2 *__restrict__ items, int64_t n_items,
+                                   const int32_t *__restrict__ cell_start, int min_cnt, int2 *__restrict__ out_a,
+                                   uint32_t *__restrict__ n_a, int2 *__restrict__ out_b, uint32_t *__restrict__ n_b) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n_items;
+    int2 it = make_int2(0, 0);
+    bool a = false;
+    if (valid) {
+        it = items[i];
+        a = min(kTile, cell_start[it.x + 1] - it.y) >= min_cnt;
+    }
+    const unsigned ma = __ballot_sync(kFull, valid && a), mb = __ballot_sync(kFull, valid && !a);
+    const int lane = threadIdx.x & 31;
+    uint32_t ba = 0, bb = 0;
+    if (lane == 0) {
+        if (ma) ba = atomicAdd(n_a, (uint32_t)__popc(ma));
+        if (mb) bb = atomicAdd(n_b, (uint32_t)__popc(mb));
+    }
+    ba = __shfl_sync(kFull, ba, 0);
+    bb = __shfl_sync(kFull, bb, 0);
+    if (valid) {
+        if (a) out_a[ba + __popc(ma & lanemask_lt())] = it;
+        else out_b[bb + __popc(mb & lanemask_lt())] = it;
+    }
+}
+
 __global__ void item_count_kernel(const int32_t *__restrict__ cell_start, int64_t n_cells,
                                   uint32_t *__restrict__ cnt) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -423,6 +452,24 @@ struct RowTable {
     int off[kWarp + 1];  // exclusive prefix of the row lengths; off[n_rows] = total
 };
 
+// Row table from one (start, len) range per lane (lanes >= n_rows hold len 0).
+__device__ __forceinline__ int build_rows(int start, int len, int n_rows, RowTable &rt, int lane) {
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane < n_rows) {
+        rt.start[lane] = start;
+        rt.off[lane] = incl - len;
+    }
+    const int total = __shfl_sync(kFull, incl, kWarp - 1);
+    if (lane == 0) rt.off[n_rows] = total;
+    __syncwarp();
+    return total;
+}
+
 // CELLS: ranges of cell indices >= min_cell; otherwise ranges of point indices.
 template <bool CELLS>
 __device__ __forceinline__ int gather_rows(const int2 *__restrict__ nbr_row, int n_rows,
@@ -439,20 +486,7 @@ __device__ __forceinline__ int gather_rows(const int2 *__restrict__ nbr_row, int
             len = cell_start[cr.y] - start;
         }
     }
-    int incl = len;
-#pragma unroll
-    for (int o = 1; o < kWarp; o <<= 1) {
-        const int y = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane < n_rows) {
-        rt.start[lane] = start;
-        rt.off[lane] = incl - len;
-    }
-    const int total = __shfl_sync(kFull, incl, kWarp - 1);
-    if (lane == 0) rt.off[n_rows] = total;
-    __syncwarp();
-    return total;
+    return build_rows(start, len, n_rows, rt, lane);
 }
 
 // Candidate t (0 <= t < total) of the flattened rows: the last row whose offset is <= t.
@@ -483,13 +517,14 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts,
     int dense_skip, int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap,
     int list_stride, unsigned long long *__restrict__ pair_counter, const JobDev *__restrict__ jobs,
-    const int32_t *__restrict__ cell_job) {
+    const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ RowTable s_rows[kWarpsPerBlock];
     __shared__ int s_list[kWarpsPerBlock][kTile * kSmemListCap];
     __shared__ int s_cnt[kWarpsPerBlock][kTile];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    if (n_items_dev) n_items = *n_items_dev;  // a list whose length the device wrote
     const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     if (item_id >= n_items) return;
     const int2 item = items[item_id];
@@ -565,7 +600,9 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
     if (lane < cnt) nn_sorted[p0 + lane] = mine;
     if (nbr_list && smem_list) {
         __syncwarp();
-        if (lane < cnt && mine < min_pts) {
+        // point units keep every point's list (the union starts from the cores'
+        // lists); cell units only need the lists of the points below min_pts
+        if (lane < cnt && (!dense_skip || mine < min_pts)) {
             const int len = min(mine, list_cap);
             for (int q = 0; q < len; ++q) nbr_list[(int64_t)(p0 + lane) * list_stride + q] = sl[lane * kSmemListCap + q];
         }
@@ -892,12 +929,14 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2,
     const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core,
     int32_t *parent, unsigned long long *__restrict__ pair_counter, int *err, const JobDev *__restrict__ jobs,
-    const int32_t *__restrict__ cell_job) {
+    const int32_t *__restrict__ cell_job, const int32_t *__restrict__ cell_root) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ int s_idx[kWarpsPerBlock][kTile];
     __shared__ int s_root[kWarpsPerBlock][kTile];
     __shared__ RowTable s_rows[kWarpsPerBlock];
+    __shared__ RowTable s_cells[kWarpsPerBlock];
+    __shared__ int s_need[kWarpsPerBlock][kWarp];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     if (item_id >= n_items) return;
@@ -912,7 +951,48 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
     RowTable &rt = s_rows[wib];
     const int nc = load_item_cores<D>(xs, core_sorted, p0, cnt, true, si, sidx, lane);
     if (nc == 0) return;
-    const int total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
+    // Cell-level pass (cell_root: the one root of each cell's cores, -2 when they
+    // differ, -1 without cores; taken after the list unions).  When the item's
+    // cores share root r, every candidate cell whose cores all hang under r is
+    // already joined to the item and is skipped whole; only the remaining cells'
+    // points are scanned.  A stale cell root (a root since hooked elsewhere) only
+    // makes a cell scanned, never skipped.
+    int total = -1, rows = n_rows;
+    if (cell_root) {
+        const int myroot = lane < nc ? uf_find(parent, sidx[lane], err) : -1;
+        const int root0 = __shfl_sync(kFull, myroot, 0);
+        if (__all_sync(kFull, lane >= nc || myroot == root0)) {
+            RowTable &rc = s_cells[wib];
+            const int tcells = gather_rows<true>(nbr + (int64_t)A * n_rows, n_rows, cell_start, A, rc, lane);
+            int n_need = 0;
+            bool overflow = false;
+            for (int cb = 0; cb < tcells; cb += kWarp) {
+                const int t = cb + lane;
+                const int c = t < tcells ? row_lookup(rc, n_rows, t) : -1;
+                const bool need = c >= 0 && cell_has_core[c] && __ldg(cell_root + c) != root0;
+                const unsigned m = __ballot_sync(kFull, need);
+                if (n_need + __popc(m) > kWarp) {
+                    overflow = true;
+                    break;
+                }
+                if (need) s_need[wib][n_need + __popc(m & lanemask_lt())] = c;
+                n_need += __popc(m);
+            }
+            __syncwarp();
+            if (!overflow) {
+                if (n_need == 0) return;
+                int start = 0, len = 0;
+                if (lane < n_need) {
+                    const int c = s_need[wib][lane];
+                    start = cell_start[c];
+                    len = cell_start[c + 1] - start;
+                }
+                total = build_rows(start, len, n_need, rt, lane);
+                rows = n_need;
+            }
+        }
+    }
+    if (total < 0) total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
     unsigned long long pairs = 0;
     for (int tb = 0; tb < total; tb += kWarp) {
         // roots of the item's cores, refreshed every chunk so that candidates already
@@ -925,7 +1005,7 @@ __global__ void __launch_bounds__(kBlock) union_points_kernel(
         __syncwarp();
         const int t = tb + lane;
         int j = -1;
-        if (t < total) j = row_lookup(rt, n_rows, t);
+        if (t < total) j = row_lookup(rt, rows, t);
         bool valid = j > p0 && core_sorted[j];
         float xj[D];
         int pj = -1;
@@ -980,6 +1060,51 @@ __global__ void comp_min_kernel(int64_t nv, const uint8_t *__restrict__ core_sor
         const int m = (int)__reduce_min_sync(kFull, mine ? (unsigned)r : (unsigned)kNoCluster);
         if (lane == leader) atomicMin(comp_min + lroot, m);
         pending &= ~__ballot_sync(kFull, mine);
+    }
+}
+
+// The one root of each cell's cores (parent flattened): -1 without cores, -2 when
+// they do not all share it.
+__global__ void cell_root_kernel(int64_t n_cells, const int32_t *__restrict__ cell_start,
+                                 const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core,
+                                 const int32_t *__restrict__ parent, int32_t *__restrict__ cell_root) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    int r = -1;
+    if (cell_has_core[c]) {
+        const int e = cell_start[c + 1];
+        for (int p = cell_start[c]; p < e; ++p) {
+            if (!core_sorted[p]) continue;
+            const int q = parent[p];
+            if (r == -1) r = q;
+            else if (q != r) {
+                r = -2;
+                break;
+            }
+        }
+    }
+    cell_root[c] = r;
+}
+
+// Point units, first step of the union: every core is joined to the cores among
+// the first neighbours the count recorded for it (at most kListUnions of them; no
+// distance test, each listed point is in range).  Clusters are then nearly all
+// linked, and the candidate scan that follows skips every candidate whose root is
+// already its item's.
+constexpr int kListUnions = 8;
+__global__ void union_lists_kernel(int64_t nv, const int32_t *__restrict__ nn_sorted,
+                                   const int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
+                                   const uint8_t *__restrict__ core_sorted, int32_t *parent, int *err,
+                                   const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job,
+                                   const int32_t *__restrict__ pcell) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nv || !core_sorted[s]) return;
+    const int cap = jobs ? jobs[cell_job[pcell[s]]].list_cap : list_cap;
+    const int len = min(min(nn_sorted[s], cap), kListUnions);
+    const int32_t *l = nbr_list + s * list_stride;
+    for (int q = 0; q < len; ++q) {
+        const int j = l[q];
+        if (j != (int)s && core_sorted[j]) uf_union(parent, (int)s, j, err);
     }
 }
 

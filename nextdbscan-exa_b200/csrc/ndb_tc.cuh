@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
     int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
     unsigned long long *__restrict__ pair_counter, unsigned long long *__restrict__ band_counter,
     unsigned int *__restrict__ work, int *__restrict__ err, const JobDev *__restrict__ jobs,
-    const int32_t *__restrict__ cell_job) {
+    const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr) {
     constexpr int KP = KPad<D>::v, P = Stride<D>::P, KC = KP / 4;
     __shared__ __align__(1024) uint32_t s_a[2][2][KC * kM * 4];  // [buffer][hi, lo] candidate tiles
     __shared__ __align__(128) uint32_t s_b[2][KC * kN * 4];      // [hi, lo] the item's points
@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = s_tmem;
+    if (n_items_dev) n_items = *n_items_dev;  // a list whose length the device wrote
     uint32_t phase = 0, pending = 0;  // per buffer: parity of its next completion; MMAs not yet waited for
     unsigned long long pairs = 0, band = 0;
     const float kap = kappa<KP>();

@@ -97,6 +97,7 @@ class NdbStats(ctypes.Structure):
         ("solo_jobs", ctypes.c_int32),
         ("tensor_filter", ctypes.c_int32),
         ("band_pairs", ctypes.c_int64),
+        ("tensor_items", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:
