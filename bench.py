@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=50_000, help="points in the bounded CPU sample")
     ap.add_argument("--jobs", type=int, default=4096, help="jobs of the batched configuration 4")
+    ap.add_argument("--count-kernel", choices=["auto", "exact", "tensor"], default="auto",
+                    help="neighbour-count kernel for d >= 8: picked per item (auto), exact FP32 only, or tensor filter")
     ap.add_argument("--no-plain", action="store_true", help="configuration 4: skip the one-call-per-job form")
     return ap.parse_args()
 
@@ -275,8 +277,11 @@ def run_ours(args):
     full = args.full_count
     torch.cuda.synchronize()
 
+    ck_kw = {"exact": {"exact_count": True}, "tensor": {"tensor_filter": True}}.get(args.count_kernel, {})
+
     def step():
-        return ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(), full_count=full)
+        return ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(), full_count=full,
+                              **ck_kw)
 
     for _ in range(args.warmup):
         step()
@@ -338,7 +343,7 @@ def run_ours(args):
         hci = torch.empty(n, dtype=torch.int32).pin_memory()
         for _ in range(2):
             ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
-                         full_count=full)
+                         full_count=full, **ck_kw)
         torch.cuda.synchronize()
         barrier(world)
         e_ms = []
@@ -348,7 +353,7 @@ def run_ours(args):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
-                         full_count=full)
+                         full_count=full, **ck_kw)
             e1.record(stream)
             e1.synchronize()
             e_ms.append(e0.elapsed_time(e1))
@@ -368,6 +373,9 @@ def run_ours(args):
     s0 = stats[-1]
     dominant = max(kern, key=kern.get)
     roof = roofline(dominant, kern[dominant], s0, n, hbm_peak, peak_src, clk_sum)
+    tkey = "tensor_count_kernel" if (dominant == "count_kernel" and s0["tensor_items"]) else dominant
+    roof["traffic"] = traffic_per_launch(w.name, tkey, n)
+    roof["traffic_source"] = "profiles/traffic_per_launch.md (ncu capture, scaled by n)" if roof["traffic"] else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -451,7 +459,8 @@ def run_ours_batch(args):
             arr[k].cluster_index_out = cip + 4 * int(poff[k])
         return arr
 
-    full = lib.FLAG_FULL_COUNT if args.full_count else 0
+    full = (lib.FLAG_FULL_COUNT if args.full_count else 0) | {"exact": lib.FLAG_EXACT_COUNT,
+                                                              "tensor": lib.FLAG_TENSOR_FILTER}.get(args.count_kernel, 0)
     dev_jobs = job_table(x.data_ptr(), nn.data_ptr(), ci.data_ptr())
     torch.cuda.synchronize()
 
@@ -591,6 +600,20 @@ def run_ours_batch(args):
     return 0
 
 
+def traffic_per_launch(workload: str, kernel: str, n: int):
+    """DRAM bytes per launch of kernel on workload, from the committed ncu captures
+    (profiles/traffic_per_launch.md), scaled by points; None when not captured."""
+    p = os.path.join(ROOT, "profiles", "traffic_per_launch.md")
+    try:
+        for line in open(p):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) >= 4 and cells[0] == workload and cells[1] == kernel and cells[2].isdigit():
+                return int(cells[3]) * n / int(cells[2])
+    except OSError:
+        pass
+    return None
+
+
 def count_launches(s) -> int:
     """Kernels of one job, as counted by the library at every launch site."""
     return int(s["kernel_launches"])
@@ -606,6 +629,14 @@ def roofline(kind, ms, s, n, hbm_peak, peak_src, clk):
         return {"kernel": "radix_sort (all passes)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
                 "peak_source": f"{peak_src} hbm_gbs"}
+    if kind == "union_kernel":
+        # union-find over random parents: 8 bytes per tested core pair (two parent
+        # reads) + 12 per point (core flag, parent write, label write)
+        ab = 8 * s["union_pairs"] + 12 * s["n_valid"]
+        achieved = ab / (ms / 1000.0) / 1e9
+        return {"kernel": "union (main kernel)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "peak_source": f"{peak_src} hbm_gbs", "work": f"{ab} algorithmic bytes"}
     pairs = {"count_kernel": s["count_pairs"], "union_kernel": s["union_pairs"],
              "border_kernel": s["border_pairs"]}[kind]
     pair_dims = {"count_kernel": s["count_pair_dims"], "union_kernel": s["union_pair_dims"],

@@ -103,7 +103,7 @@ typedef struct ndb_stats {
     float ms_border;          /* device time of the border assignment + meta */
     float ms_sort_kernels;    /* device time of the radix sort (all passes) */
     float ms_count_kernel;    /* device time of the neighbour-count kernel */
-    float ms_union_kernel;    /* device time of the union-find kernel */
+    float ms_union_kernel;    /* device time of the main union kernel (cells, or points after the list unions) */
     float ms_border_kernel;   /* device time of the border kernel */
     int32_t sort_passes;      /* radix passes (8 bits each) */
     int32_t key_bytes;        /* 4 or 8 */

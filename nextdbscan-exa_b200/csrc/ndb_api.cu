@@ -351,17 +351,20 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
 template <int D>
 void count_phase(ndb_ctx *ctx);
 
-// The tensor-core filter's preconditions: d at or above the threshold (8 unless
-// NDB_TC_MIN_DIM raises it), the eps grid (row tables of <= 32 rows), eps^2 a
+// The tensor-core filter's preconditions: d >= 8 (and, unless NDB_FLAG_TENSOR_FILTER
+// asks for it, d at or above the automatic threshold: 12 by measurement on B200,
+// where the filter beats the exact kernel on full items at d = 16 but not at d = 8;
+// NDB_TC_MIN_DIM overrides), the eps grid (row tables of <= 32 rows), eps^2 a
 // normal float far from under- and overflow, and coordinates within +-2^60 so that
 // no centred difference or squared norm overflows.  Results never depend on it.
 inline bool tc_eligible(int d, float e2, const double *lo, const double *hi, bool linked, int n_rows,
                         uint32_t flags) {
-    static const int min_dim = [] {
+    static const int auto_min_dim = [] {
         const char *s = getenv("NDB_TC_MIN_DIM");
-        const int v = s ? atoi(s) : tc::kMinDim;
+        const int v = s ? atoi(s) : 12;
         return v < tc::kMinDim ? tc::kMinDim : v;
     }();
+    const int min_dim = (flags & NDB_FLAG_TENSOR_FILTER) ? tc::kMinDim : auto_min_dim;
     if (d < min_dim || (flags & NDB_FLAG_EXACT_COUNT) || linked || n_rows > kWarp) return false;
     if (!(e2 >= 0x1p-100f && e2 <= 0x1p100f)) return false;
     for (int a = 0; a < d; ++a)
@@ -526,7 +529,7 @@ void labels_phase(ndb_ctx *ctx) {
     ck(ctx, cudaGetLastError());
 
     const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
-    cudaEventRecord(ctx->kev[4], st);
+    cudaEventRecord(ctx->kev[4], st);  // moved to the main union kernel below when there is one
     if (ctx->n_items > 0) {
         if (ctx->cell_units) {
             if (ctx->key64)
@@ -543,6 +546,7 @@ void labels_phase(ndb_ctx *ctx) {
                     ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
             ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                       n_units, err);
+            cudaEventRecord(ctx->kev[4], st);
             ++launch_counter(), union_cells_kernel<D><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
                 n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->xs.as<float>(),
                 ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
@@ -559,6 +563,7 @@ void labels_phase(ndb_ctx *ctx) {
             ++launch_counter(), cell_root_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
                 n_cells, ctx->cell_start.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
                 ctx->parent.as<int32_t>(), ctx->cell_cid.as<int32_t>());
+            cudaEventRecord(ctx->kev[4], st);
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                 ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),

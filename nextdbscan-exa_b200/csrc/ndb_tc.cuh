@@ -33,7 +33,7 @@ constexpr int kN = 32;               // points of one item: MMA N, TMEM columns 
 constexpr int kThreads = 128;        // four warps, one per TMEM lane quadrant
 constexpr uint32_t kTmemCols = 64;   // two accumulator buffers
 constexpr uint32_t kWaitLimit = 1u << 22;
-constexpr int kMinDim = 8;           // default: the tensor filter runs for d >= 8
+constexpr int kMinDim = 8;           // the kernel is built for d >= 8 (K padded to 8 or 16)
 
 template <int D>
 struct KPad {
