@@ -123,13 +123,23 @@ def dist_env():
 
 
 def max_over_ranks(val: float, world: int) -> float:
+    """Largest value over the ranks (timing: the slowest rank sets the job time).
+    NCCL groups reduce a device tensor, gloo groups (CPU tests) a host one."""
     if world == 1:
         return val
     import torch
     import torch.distributed as dist
-    t = torch.tensor([val], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([val], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, steps: int, local_ms: float, world: int) -> tuple[float, float]:
+    """Replicas: every rank processes units_per_rank per step; the whole job's rate
+    is all ranks' units over the slowest rank's device time."""
+    total_ms = max_over_ranks(local_ms, world)
+    return world * units_per_rank * steps / (total_ms / 1000.0), total_ms
 
 
 def barrier(world: int):
@@ -303,8 +313,7 @@ def run_ours(args):
             stats.append(ctx.stats())
     torch.cuda.synchronize()
     barrier(world)
-    total_ms = max_over_ranks(sum(step_ms), world)
-    value = world * n * args.steps / (total_ms / 1000.0)
+    value, total_ms = whole_job_rate(n, args.steps, sum(step_ms), world)
 
     # d >= 8: the plain GPU form (exact FP32 count kernel) and the tensor-core filtered
     # form beside the default (the library picks between them by tile fill)
@@ -488,8 +497,7 @@ def run_ours_batch(args):
             stats.append(ctx.stats())
     torch.cuda.synchronize()
     barrier(world)
-    total_ms = max_over_ranks(sum(step_ms), world)
-    value = world * total * args.steps / (total_ms / 1000.0)
+    value, total_ms = whole_job_rate(total, args.steps, sum(step_ms), world)
     h_ci = ci.cpu().numpy()
     clusters = sum(int(dev_jobs[k].result.clusters) for k in range(nj))
     noise = sum(int(dev_jobs[k].result.noise) for k in range(nj))

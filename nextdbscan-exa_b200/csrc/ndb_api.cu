@@ -560,9 +560,10 @@ void labels_phase(ndb_ctx *ctx) {
                 ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                           n_units, err);
             }
-            ++launch_counter(), cell_root_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
-                n_cells, ctx->cell_start.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                ctx->parent.as<int32_t>(), ctx->cell_cid.as<int32_t>());
+            ck(ctx, cudaMemsetAsync(ctx->cell_cid.ptr, 0xff, (size_t)n_cells * sizeof(int32_t), st));  // -1
+            ++launch_counter(), cell_root_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+                nv, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(),
+                ctx->cell_cid.as<int32_t>());
             cudaEventRecord(ctx->kev[4], st);
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
@@ -1169,9 +1170,10 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
                 ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                           n_units, err);
             }
-            ++launch_counter(), cell_root_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
-                n_cells, ctx->cell_start.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-                ctx->parent.as<int32_t>(), ctx->cell_cid.as<int32_t>());
+            ck(ctx, cudaMemsetAsync(ctx->cell_cid.ptr, 0xff, (size_t)n_cells * sizeof(int32_t), st));  // -1
+            ++launch_counter(), cell_root_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+                nv, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(),
+                ctx->cell_cid.as<int32_t>());
             ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
                 ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
                 ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
@@ -1385,6 +1387,31 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
     int bits = 1;
     while (bits < 64 && ldexp(1.0, bits) - 1.0 < (double)key_base) ++bits;
     bp.key_bits = bits;
+    // keys past 32 bits: split into pipelines whose cells fit 32-bit keys (one sort
+    // pass fewer, half the hash table) as long as every part keeps more than one job
+    if (bits > 32 && nj > 1) {
+        const unsigned long long limit = (1ull << 32) - 1;  // room for the invalid key
+        std::vector<int> part;
+        unsigned long long acc = 0;
+        bool split_ok = true;
+        std::vector<std::vector<int>> parts;
+        for (int m = 0; m < nj; ++m) {
+            const unsigned long long cells = (m + 1 < nj ? bp.jd[m + 1].key_base : key_base) - bp.jd[m].key_base;
+            if (cells >= limit) split_ok = false;
+            if (!part.empty() && acc + cells >= limit) {
+                parts.push_back(part);
+                part.clear();
+                acc = 0;
+            }
+            part.push_back(members[m]);
+            acc += cells;
+        }
+        parts.push_back(part);
+        if (split_ok && parts.size() > 1) {
+            for (auto &pm : parts) run_group<D>(ctx, jobs, pm, flags, solo);
+            return;
+        }
+    }
     if (getenv("NDB_DEBUG")) {
         for (int m = 0; m < nj; ++m)
             fprintf(stderr, "ndb batch d=%d job %d: off=%lld n=%lld invalid=%llu key_base=%llu k=%d\n", D, members[m],

@@ -1064,26 +1064,20 @@ __global__ void comp_min_kernel(int64_t nv, const uint8_t *__restrict__ core_sor
 }
 
 // The one root of each cell's cores (parent flattened): -1 without cores, -2 when
-// they do not all share it.
-__global__ void cell_root_kernel(int64_t n_cells, const int32_t *__restrict__ cell_start,
-                                 const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core,
-                                 const int32_t *__restrict__ parent, int32_t *__restrict__ cell_root) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n_cells) return;
-    int r = -1;
-    if (cell_has_core[c]) {
-        const int e = cell_start[c + 1];
-        for (int p = cell_start[c]; p < e; ++p) {
-            if (!core_sorted[p]) continue;
-            const int q = parent[p];
-            if (r == -1) r = q;
-            else if (q != r) {
-                r = -2;
-                break;
-            }
-        }
-    }
-    cell_root[c] = r;
+// they do not all share it.  One thread per point: the first core of a cell to
+// arrive installs its root, any core with another root marks the cell mixed; a
+// core whose root is already there skips the atomic.  cell_root starts at -1.
+__global__ void cell_root_kernel(int64_t nv, const int32_t *__restrict__ pcell,
+                                 const uint8_t *__restrict__ core_sorted, const int32_t *__restrict__ parent,
+                                 int32_t *cell_root) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nv || !core_sorted[s]) return;
+    const int c = pcell[s];
+    const int r = parent[s];
+    const int cur = __ldcg(cell_root + c);
+    if (cur == r || cur == -2) return;
+    const int old = cur == -1 ? atomicCAS(cell_root + c, -1, r) : cur;
+    if (old != -1 && old != r) atomicExch(cell_root + c, -2);
 }
 
 // Point units, first step of the union: every core is joined to the cores among

@@ -136,3 +136,24 @@ def test_batched_cluster_roots_match_reference_labels(ctx):
     for (name, g), (nn, ci, res) in zip(probs, outs):
         ids = np.unique(ci[ci != 2**31 - 1])
         np.testing.assert_array_equal(ids, roots_of(g["cluster_label"]), err_msg=name)
+
+
+def test_batch_split_to_keep_32_bit_keys(ctx, pkg):
+    """Jobs whose cells add up past 2^32 keys run as several pipelines with 32-bit
+    keys; the results are still those of one run per job."""
+    rng = np.random.default_rng(41)
+    probs = []
+    for k in range(3):  # about 1.5e9 cells each (3-D, extent 661, eps 1)
+        x = rng.uniform(0, 661, (2000, 3)).astype(np.float32)
+        x[:200] = (rng.normal(300, 0.4, (200, 3))).astype(np.float32)
+        probs.append((x, 1.0, 4))
+    a = load_golden("blobs_d3")
+    probs.append((a["coords"], float(a["eps"]), int(a["min_pts"])))
+    outs = ctx.run_batched(probs, full_count=True)
+    s = ctx.stats()
+    assert s["pipelines"] >= 2 and s["key_bits"] <= 32 and s["solo_jobs"] == 0
+    for k, ((x, e, m), (nn, ci, res)) in enumerate(zip(probs, outs)):
+        nn1, ci1, res1 = ctx.run(x, e, m, full_count=True)
+        np.testing.assert_array_equal(nn, nn1, err_msg=f"job {k}")
+        np.testing.assert_array_equal(ci, ci1, err_msg=f"job {k}")
+        assert res == res1, k
