@@ -352,9 +352,9 @@ template <int D>
 void count_phase(ndb_ctx *ctx);
 
 // The tensor-core filter's preconditions: d >= 8 (and, unless NDB_FLAG_TENSOR_FILTER
-// asks for it, d at or above the automatic threshold: 12 by measurement on B200,
-// where the filter beats the exact kernel on full items at d = 16 but not at d = 8;
-// NDB_TC_MIN_DIM overrides), the eps grid (row tables of <= 32 rows), eps^2 a
+// asks for it or counts are full, d at or above the automatic threshold: 12 by
+// measurement on B200, where with early exit the filter beats the exact kernel on
+// full items at d = 16 but not at d = 8; NDB_TC_MIN_DIM overrides), the eps grid (row tables of <= 32 rows), eps^2 a
 // normal float far from under- and overflow, and coordinates within +-2^60 so that
 // no centred difference or squared norm overflows.  Results never depend on it.
 inline bool tc_eligible(int d, float e2, const double *lo, const double *hi, bool linked, int n_rows,
@@ -364,7 +364,9 @@ inline bool tc_eligible(int d, float e2, const double *lo, const double *hi, boo
         const int v = s ? atoi(s) : 12;
         return v < tc::kMinDim ? tc::kMinDim : v;
     }();
-    const int min_dim = (flags & NDB_FLAG_TENSOR_FILTER) ? tc::kMinDim : auto_min_dim;
+    // full counts scan every candidate of every point, so the tiles stay full: there
+    // the filter measured 1.17x the exact kernel already at d = 8
+    const int min_dim = (flags & (NDB_FLAG_TENSOR_FILTER | NDB_FLAG_FULL_COUNT)) ? tc::kMinDim : auto_min_dim;
     if (d < min_dim || (flags & NDB_FLAG_EXACT_COUNT) || linked || n_rows > kWarp) return false;
     if (!(e2 >= 0x1p-100f && e2 <= 0x1p100f)) return false;
     for (int a = 0; a < d; ++a)
