@@ -247,6 +247,14 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 // ---------------------------------------------------------------------------
 // phase 1
 // ---------------------------------------------------------------------------
+// Lanes per cell of the row lookup, as log2: the stencil's row count rounded up to a
+// power of two (25 rows: one warp per cell; 5 rows: four cells per warp).
+inline int row_group_log2(int n_rows) {
+    int l = 0;
+    while ((1 << l) < n_rows) ++l;
+    return l;
+}
+
 template <int D, typename K>
 void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     cudaStream_t st = ctx->stream;
@@ -326,8 +334,9 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
     int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
     ck(ctx, cudaMemcpyAsync(rows_dev, pl.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
-    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
-        ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, ctx->hash_keys.as<K>(),
+    const int rlog = row_group_log2(n_rows);
+    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells << rlog), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, rlog, ctx->hash_keys.as<K>(),
         ctx->hash_vals.as<int32_t>(), (unsigned long long)(hsize - 1), ctx->nbr.as<int2>(), nullptr, nullptr);
     ck(ctx, cudaGetLastError());
 
@@ -437,13 +446,13 @@ void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_ite
         ex_items = rest;
         ex_n = scal + 5;
     }
-    const unsigned grid = (unsigned)((n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    const unsigned grid = (unsigned)((n_items + kCountWarps - 1) / kCountWarps);
     if (early)
-        ++launch_counter(), count_kernel<D, true><<<grid, kBlock, 0, st>>>(
+        ++launch_counter(), count_kernel<D, true><<<grid, kCountWarps * kWarp, 0, st>>>(
             ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
             list_stride, counters + 2, jobs, cell_job, ex_n);
     else
-        ++launch_counter(), count_kernel<D, false><<<grid, kBlock, 0, st>>>(
+        ++launch_counter(), count_kernel<D, false><<<grid, kCountWarps * kWarp, 0, st>>>(
             ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
             list_stride, counters + 2, jobs, cell_job, ex_n);
     ck(ctx, cudaGetLastError());
@@ -567,7 +576,8 @@ void labels_phase(ndb_ctx *ctx) {
                 nv, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(),
                 ctx->cell_cid.as<int32_t>());
             cudaEventRecord(ctx->kev[4], st);
-            ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
+            const unsigned pgrid = (unsigned)((ctx->n_items + kCountWarps - 1) / kCountWarps);
+            ++launch_counter(), union_points_kernel<D><<<pgrid, kCountWarps * kWarp, 0, st>>>(
                 ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                 ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
                 ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr, ctx->cell_cid.as<int32_t>());
@@ -1088,8 +1098,9 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
     int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
     ck(ctx, cudaMemcpyAsync(rows_dev, bp.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
-    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
-        ctx->cell_key.as<K>(), n_cells, bp.jd[0].g, rows_dev, n_rows, ctx->hash_keys.as<K>(),
+    const int rlog = row_group_log2(n_rows);
+    ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells << rlog), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, bp.jd[0].g, rows_dev, n_rows, rlog, ctx->hash_keys.as<K>(),
         ctx->hash_vals.as<int32_t>(), hmask, ctx->nbr.as<int2>(), jobs_dev, cell_job);
     ck(ctx, cudaGetLastError());
 
@@ -1176,7 +1187,8 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
             ++launch_counter(), cell_root_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
                 nv, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(),
                 ctx->cell_cid.as<int32_t>());
-            ++launch_counter(), union_points_kernel<D><<<grid, kBlock, 0, st>>>(
+            const unsigned pgrid = (unsigned)((n_items + kCountWarps - 1) / kCountWarps);
+            ++launch_counter(), union_points_kernel<D><<<pgrid, kCountWarps * kWarp, 0, st>>>(
                 ctx->items.as<int2>(), n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows,
                 ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
                 ctx->parent.as<int32_t>(), counters + 3, err, jobs_dev, cell_job, ctx->cell_cid.as<int32_t>());

@@ -80,6 +80,9 @@ constexpr int kMaxRowCells = 5;
 constexpr int kMaxListCap = 64;  // largest min_pts - 1 for which neighbour lists are kept
 constexpr int kSmemListCap = 16;  // lists up to this length are staged in shared memory  // cells per stencil row looked up together (2*xr+1 <= 5)
 constexpr int kWarpsPerBlock = kBlock / kWarp;
+// The count runs two warps per block: an item's candidate list can be thousands of
+// points long, and small blocks free their slot as soon as both items are done.
+constexpr int kCountWarps = 2;
 
 // ---------------------------------------------------------------------------
 // point validity: a point takes part in the grid iff all coordinates are finite
@@ -340,15 +343,19 @@ __device__ __forceinline__ void decode_key(K key, const GridDev &g, long long &x
 template <typename K>
 __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell_key, int64_t n_cells,
                                                       GridDev g_one, const int4 *__restrict__ rows, int n_rows,
-                                                      const K *__restrict__ hkeys, const int32_t *__restrict__ hvals,
-                                                      unsigned long long mask, int2 *__restrict__ nbr,
-                                                      const JobDev *__restrict__ jobs,
+                                                      int group_log2, const K *__restrict__ hkeys,
+                                                      const int32_t *__restrict__ hvals, unsigned long long mask,
+                                                      int2 *__restrict__ nbr, const JobDev *__restrict__ jobs,
                                                       const int32_t *__restrict__ cell_job) {
+    // one lane per (cell, row): 2^group_log2 lanes (>= n_rows) per cell, so
+    // a cell's rows are looked up in parallel and its row table is written at once
     __shared__ int4 s_rows[kMaxRows];
     for (int r = threadIdx.x; r < n_rows; r += blockDim.x) s_rows[r] = rows[r];
     __syncthreads();
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n_cells) return;
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t c = gid >> group_log2;
+    const int r = (int)(gid & ((1 << group_log2) - 1));
+    if (c >= n_cells || r >= n_rows) return;
     unsigned long long key_base = 0;
     GridDev g = g_one;
     if (jobs) {
@@ -358,41 +365,44 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
     }
     long long cc[kMaxGridDims];
     decode_key<K>((K)((unsigned long long)cell_key[c] - key_base), g, cc);
-    int2 *out = nbr + c * n_rows;
-    for (int r = 0; r < n_rows; ++r) {
-        const int4 row = s_rows[r];
-        const int off[kMaxGridDims] = {0, row.x, row.y, row.z};
-        bool in = true;
-        unsigned long long base = key_base;
+    const int4 row = s_rows[r];
+    const int off[kMaxGridDims] = {0, row.x, row.y, row.z};
+    bool in = true;
+    unsigned long long base = key_base;
 #pragma unroll
-        for (int a = 1; a < kMaxGridDims; ++a) {
-            if (a < g.k) {
-                const long long v = cc[a] + off[a];
-                in = in && v >= 0 && v < g.g[a];
-                base += (unsigned long long)(v < 0 ? 0 : v) * g.stride[a];
-            }
+    for (int a = 1; a < kMaxGridDims; ++a) {
+        if (a < g.k) {
+            const long long v = cc[a] + off[a];
+            in = in && v >= 0 && v < g.g[a];
+            base += (unsigned long long)(v < 0 ? 0 : v) * g.stride[a];
         }
-        int2 res = make_int2(0, 0);
-        if (in) {
-            const long long x0 = cc[0] - row.w < 0 ? 0 : cc[0] - row.w;
-            const long long x1 = cc[0] + row.w > g.g[0] - 1 ? g.g[0] - 1 : cc[0] + row.w;
-            // the row's existing cells are consecutive in the sorted cell list: find the
-            // first one by hashing (usually the first probe, at x0), then walk the keys
-            int ca = -1;
-            for (long long xx = x0; xx <= x1 && ca < 0; ++xx)
-                ca = hash_find(hkeys, hvals, mask, base + (unsigned long long)xx);
-            int lo = 0x7fffffff, hi = -1;
-            if (ca >= 0) {
-                const unsigned long long kmax = base + (unsigned long long)x1;
-                int cb = ca + 1;
-                while (cb < n_cells && (unsigned long long)__ldg(cell_key + cb) <= kmax) ++cb;
-                lo = ca;
-                hi = cb - 1;
-            }
-            if (hi >= 0) res = make_int2(lo, hi + 1);
-        }
-        out[r] = res;
     }
+    int2 res = make_int2(0, 0);
+    if (in) {
+        const long long x0 = cc[0] - row.w < 0 ? 0 : cc[0] - row.w;
+        const long long x1 = cc[0] + row.w > g.g[0] - 1 ? g.g[0] - 1 : cc[0] + row.w;
+        // the row's existing cells are consecutive in the sorted cell list: find the
+        // first one by hashing (usually the first probe, at x0), then count the keys
+        // that follow it within the row (independent loads, at most 2 row.w of them)
+        int ca = -1;
+        for (long long xx = x0; xx <= x1 && ca < 0; ++xx) ca = hash_find(hkeys, hvals, mask, base + (unsigned long long)xx);
+        if (ca >= 0) {
+            // keys are sorted and unique: the row's cells after ca are a prefix of the
+            // next keys; four independent loads cover rows of up to 5 cells
+            const unsigned long long kmax = base + (unsigned long long)x1;
+            K nk[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) nk[q] = ca + 1 + q < n_cells ? __ldg(cell_key + ca + 1 + q) : ~(K)0;
+            int cb = ca + 1;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (cb == ca + 1 + q && ca + 1 + q < n_cells && (unsigned long long)nk[q] <= kmax) ++cb;
+            if (cb == ca + 5)
+                while (cb < n_cells && (unsigned long long)__ldg(cell_key + cb) <= kmax) ++cb;
+            res = make_int2(ca, cb);
+        }
+    }
+    nbr[c * n_rows + r] = res;
 }
 
 // Items into two lists: those with at least min_cnt points (full tiles: the
@@ -512,20 +522,19 @@ __device__ __forceinline__ int row_lookup(const RowTable &rt, int n_rows, int t)
 // points need no test at all; they report the cell size.
 // ---------------------------------------------------------------------------
 template <int D, bool EARLY>
-__global__ void __launch_bounds__(kBlock) count_kernel(
+__global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts,
     int dense_skip, int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap,
     int list_stride, unsigned long long *__restrict__ pair_counter, const JobDev *__restrict__ jobs,
     const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr) {
     constexpr int P = Stride<D>::P;
-    __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
-    __shared__ RowTable s_rows[kWarpsPerBlock];
-    __shared__ int s_list[kWarpsPerBlock][kTile * kSmemListCap];
-    __shared__ int s_cnt[kWarpsPerBlock][kTile];
+    __shared__ __align__(16) float s_i[kCountWarps][kTile * P];
+    __shared__ RowTable s_rows[kCountWarps];
+    __shared__ int s_list[kCountWarps][kTile * kSmemListCap];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     if (n_items_dev) n_items = *n_items_dev;  // a list whose length the device wrote
-    const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t item_id = (int64_t)blockIdx.x * kCountWarps + wib;
     if (item_id >= n_items) return;
     const int2 item = items[item_id];
     const int cell = item.x, p0 = item.y;
@@ -554,14 +563,14 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         store_point_smem<D>(si + lane * P, x);
     }
     const int total = gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, rt, lane);
-    // running count of each of the item's points; every lane computes the same
-    // value and writes it, so the counter needs no per-lane copy
-    int *cntk = s_cnt[wib];
-    cntk[lane] = 0;
     __syncwarp();
+    // running counts in registers: lane k holds the count of the item's point k
+    int mycnt = 0;
     unsigned long long pairs = 0;
-    // points still counting (EARLY: below min_pts); warp-uniform
+    // points still counting (EARLY: below min_pts), and points whose neighbour list
+    // is still filling (count below list_cap): both warp-uniform, updated per chunk
     unsigned act = __ballot_sync(kFull, lane < cnt);
+    unsigned lst = nbr_list && list_cap > 0 ? act : 0u;
     for (int tb = 0; tb < total; tb += kWarp) {
         const int t = tb + lane;
         const int j = t < total ? row_lookup(rt, n_rows, t) : -1;
@@ -571,32 +580,30 @@ __global__ void __launch_bounds__(kBlock) count_kernel(
         int active = 0;
         for (unsigned it = act; it; it &= it - 1) {
             const int k = __ffs(it) - 1;
-            const int ck = cntk[k];
             float xi[D];
             load_point_smem<D>(si + k * P, xi);
             const bool hit = in_range<D>(xi, xj, e2);
             const unsigned m = __ballot_sync(kFull, hit);
             // the first list_cap neighbours of each point; complete for every point
             // whose count stays below min_pts (list_cap = min_pts - 1)
-            if (nbr_list && m && ck < list_cap) {
-                const int slot = ck + __popc(m & lanemask_lt());
+            if ((lst >> k) & 1u) {
+                const int slot = __shfl_sync(kFull, mycnt, k) + __popc(m & lanemask_lt());
                 if (hit && slot < list_cap) {
                     if (smem_list) sl[k * kSmemListCap + slot] = j;
                     else nbr_list[(int64_t)(p0 + k) * list_stride + slot] = j;
                 }
             }
-            __syncwarp();
-            cntk[k] = ck + __popc(m);
+            if (lane == k) mycnt += __popc(m);
             ++active;
         }
-        __syncwarp();
         pairs += (unsigned long long)active * (unsigned long long)min(kWarp, total - tb);
+        if (lst) lst &= __ballot_sync(kFull, mycnt < list_cap);
         if (EARLY) {
-            act = __ballot_sync(kFull, lane < cnt && cntk[lane] < min_pts);
+            act = __ballot_sync(kFull, lane < cnt && mycnt < min_pts);
             if (!act) break;
         }
     }
-    const int mine = lane < cnt ? cntk[lane] : 0;
+    const int mine = lane < cnt ? mycnt : 0;
     if (lane < cnt) nn_sorted[p0 + lane] = mine;
     if (nbr_list && smem_list) {
         __syncwarp();
@@ -924,21 +931,21 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
 // predicate.
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(kBlock) union_points_kernel(
+__global__ void __launch_bounds__(kCountWarps * kWarp) union_points_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2,
     const uint8_t *__restrict__ core_sorted, const uint8_t *__restrict__ cell_has_core,
     int32_t *parent, unsigned long long *__restrict__ pair_counter, int *err, const JobDev *__restrict__ jobs,
     const int32_t *__restrict__ cell_job, const int32_t *__restrict__ cell_root) {
     constexpr int P = Stride<D>::P;
-    __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
-    __shared__ int s_idx[kWarpsPerBlock][kTile];
-    __shared__ int s_root[kWarpsPerBlock][kTile];
-    __shared__ RowTable s_rows[kWarpsPerBlock];
-    __shared__ RowTable s_cells[kWarpsPerBlock];
-    __shared__ int s_need[kWarpsPerBlock][kWarp];
+    __shared__ __align__(16) float s_i[kCountWarps][kTile * P];
+    __shared__ int s_idx[kCountWarps][kTile];
+    __shared__ int s_root[kCountWarps][kTile];
+    __shared__ RowTable s_rows[kCountWarps];
+    __shared__ RowTable s_cells[kCountWarps];
+    __shared__ int s_need[kCountWarps][kWarp];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int64_t item_id = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const int64_t item_id = (int64_t)blockIdx.x * kCountWarps + wib;
     if (item_id >= n_items) return;
     const int2 item = items[item_id];
     const int A = item.x, p0 = item.y;
