@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--count-kernel", choices=["auto", "exact", "tensor"], default="auto",
                     help="neighbour-count kernel for d >= 8: picked per item (auto), exact FP32 only, or tensor filter")
     ap.add_argument("--no-plain", action="store_true", help="configuration 4: skip the one-call-per-job form")
+    ap.add_argument("--dims", type=str, default=None,
+                    help="configuration 4: keep only the jobs of these dimensionalities (comma list)")
+    ap.add_argument("--max-jobs", type=int, default=None, help="configuration 4: keep at most this many jobs")
     return ap.parse_args()
 
 
@@ -442,6 +445,11 @@ def run_ours_batch(args):
     pkg = importlib.import_module("nextdbscan-exa_b200")
     lib = pkg.lib
     jobs = pkg.synthetic.config4(n_jobs=args.jobs)
+    if args.dims:
+        keep = {int(v) for v in args.dims.split(",")}
+        jobs = [j for j in jobs if j.d in keep]
+    if args.max_jobs:
+        jobs = jobs[:args.max_jobs]
     nj = len(jobs)
     sizes = np.array([j.n for j in jobs], np.int64)
     dims = np.array([j.d for j in jobs], np.int64)
@@ -581,7 +589,8 @@ def run_ours_batch(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator with the benchmark's distribution)",
-            "config": {"workload": "batched-4096-jobs", "jobs": nj, "points": total,
+            "config": {"workload": "batched-4096-jobs" if nj == 4096 else f"batched-subset-{nj}-jobs",
+                       "jobs": nj, "points": total,
                        "points_by_d": {int(d): int(sizes[dims == d].sum()) for d in np.unique(dims)},
                        "eps": "per job: 90th percentile of the 4-NN distance over a 1% sample",
                        "min_pts": "2d", "form": "ndb_b200_run_batched, device-resident inputs",
