@@ -571,9 +571,14 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     // is still filling (count below list_cap): both warp-uniform, updated per chunk
     unsigned act = __ballot_sync(kFull, lane < cnt);
     unsigned lst = nbr_list && list_cap > 0 ? act : 0u;
+    int row = 0;  // this lane's stencil row: its candidate index only grows
     for (int tb = 0; tb < total; tb += kWarp) {
         const int t = tb + lane;
-        const int j = t < total ? row_lookup(rt, n_rows, t) : -1;
+        int j = -1;
+        if (t < total) {
+            while (rt.off[row + 1] <= t) ++row;
+            j = rt.start[row] + (t - rt.off[row]);
+        }
         float xj[D];
         if (j >= 0) load_point<D>(xs, j, xj);
         else fill_nan<D>(xj);  // NaN fails the predicate
