@@ -499,7 +499,8 @@ __device__ __forceinline__ int gather_rows(const int2 *__restrict__ nbr_row, int
     return build_rows(start, len, n_rows, rt, lane);
 }
 
-// Candidate t (0 <= t < total) of the flattened rows: the last row whose offset is <= t.
+// Candidate t (0 <= t < total) of the flattened rows: the last row whose offset is
+// <= t.  For rows of cells (at most a few entries each).
 __device__ __forceinline__ int row_lookup(const RowTable &rt, int n_rows, int t) {
     int lo = 0, hi = n_rows - 1;
     while (lo < hi) {
@@ -508,6 +509,13 @@ __device__ __forceinline__ int row_lookup(const RowTable &rt, int n_rows, int t)
         else hi = mid - 1;
     }
     return rt.start[lo] + (t - rt.off[lo]);
+}
+
+// Candidate t for a lane whose t only grows (by a warp per step): advance the
+// lane's row cursor over the row offsets (empty rows skipped) instead of searching.
+__device__ __forceinline__ int row_next(const RowTable &rt, int &row, int t) {
+    while (rt.off[row + 1] <= t) ++row;
+    return rt.start[row] + (t - rt.off[row]);
 }
 
 // ---------------------------------------------------------------------------
@@ -574,11 +582,7 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     int row = 0;  // this lane's stencil row: its candidate index only grows
     for (int tb = 0; tb < total; tb += kWarp) {
         const int t = tb + lane;
-        int j = -1;
-        if (t < total) {
-            while (rt.off[row + 1] <= t) ++row;
-            j = rt.start[row] + (t - rt.off[row]);
-        }
+        const int j = t < total ? row_next(rt, row, t) : -1;
         float xj[D];
         if (j >= 0) load_point<D>(xs, j, xj);
         else fill_nan<D>(xj);  // NaN fails the predicate
@@ -1006,6 +1010,7 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) union_points_kernel(
     }
     if (total < 0) total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
     unsigned long long pairs = 0;
+    int cur = 0;  // this lane's stencil row
     for (int tb = 0; tb < total; tb += kWarp) {
         // roots of the item's cores, refreshed every chunk so that candidates already
         // joined to them are skipped before the predicate
@@ -1017,7 +1022,7 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) union_points_kernel(
         __syncwarp();
         const int t = tb + lane;
         int j = -1;
-        if (t < total) j = row_lookup(rt, rows, t);
+        if (t < total) j = row_next(rt, cur, t);
         bool valid = j > p0 && core_sorted[j];
         float xj[D];
         int pj = -1;
@@ -1284,10 +1289,11 @@ __global__ void __launch_bounds__(kBlock) border_kernel(
         }
     } else {
         const int total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
+        int cur = 0;
         for (int tb = 0; tb < total; tb += kWarp) {
             const int t = tb + lane;
             int j = -1;
-            if (t < total) j = row_lookup(rt, n_rows, t);
+            if (t < total) j = row_next(rt, cur, t);
             const bool valid = j >= 0 && core_sorted[j];
             float xj[D];
             int cj = kNoCluster;
