@@ -586,10 +586,16 @@ void labels_phase(ndb_ctx *ctx) {
     }
     cudaEventRecord(ctx->kev[5], st);
     ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units, err);
-    ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
-        nv, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units,
-        ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), ctx->parent.as<int32_t>(),
-        ctx->comp_min.as<int32_t>());
+    if (ctx->cell_units)
+        ++launch_counter(), comp_min_cells_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
+            n_cells, ctx->cell_start.as<int32_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->core_sorted.as<uint8_t>(),
+            ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(),
+            ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>());
+    else
+        ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+            nv, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units,
+            ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), ctx->parent.as<int32_t>(),
+            ctx->comp_min.as<int32_t>());
     ++launch_counter(), core_ids_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
         nv, ctx->core_sorted.as<uint8_t>(), ctx->pcell.as<int32_t>(), ctx->cell_units, ctx->parent.as<int32_t>(),
         ctx->comp_min.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters, nullptr, nullptr);
@@ -1197,9 +1203,16 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     }
     cudaEventRecord(ctx->kev[5], st);
     ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units, err);
-    ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
-        nv, ctx->core_sorted.as<uint8_t>(), perm, ctx->pcell.as<int32_t>(), bp.linked, ctx->core_bits.as<uint32_t>(),
-        ctx->core_prefix.as<uint32_t>(), ctx->parent.as<int32_t>(), ctx->comp_min.as<int32_t>());
+    if (bp.linked)
+        ++launch_counter(), comp_min_cells_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
+            n_cells, ctx->cell_start.as<int32_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->core_sorted.as<uint8_t>(),
+            perm, ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), ctx->parent.as<int32_t>(),
+            ctx->comp_min.as<int32_t>());
+    else
+        ++launch_counter(), comp_min_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+            nv, ctx->core_sorted.as<uint8_t>(), perm, ctx->pcell.as<int32_t>(), bp.linked,
+            ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), ctx->parent.as<int32_t>(),
+            ctx->comp_min.as<int32_t>());
     ++launch_counter(), core_ids_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
         nv, ctx->core_sorted.as<uint8_t>(), ctx->pcell.as<int32_t>(), bp.linked, ctx->parent.as<int32_t>(),
         ctx->comp_min.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters, cell_job, jc);

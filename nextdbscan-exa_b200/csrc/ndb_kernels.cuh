@@ -1080,6 +1080,37 @@ __global__ void comp_min_kernel(int64_t nv, const uint8_t *__restrict__ core_sor
     }
 }
 
+// Cell units: the smallest core rank of a cell is its first core's, because the
+// stable radix sort (started from the identity permutation) keeps the points of a
+// cell in input order.  One thread per cell instead of one per point: far fewer
+// atomics on the roots of large clusters.  Lanes sharing a root combine first.
+__global__ void comp_min_cells_kernel(int64_t n_cells, const int32_t *__restrict__ cell_start,
+                                      const uint8_t *__restrict__ cell_has_core,
+                                      const uint8_t *__restrict__ core_sorted, const int32_t *__restrict__ perm,
+                                      const uint32_t *__restrict__ core_bits,
+                                      const uint32_t *__restrict__ core_prefix, const int32_t *__restrict__ parent,
+                                      int32_t *__restrict__ comp_min) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = c < n_cells && cell_has_core[c];
+    int root = -1, r = kNoCluster;
+    if (ok) {
+        int p = cell_start[c];
+        while (!core_sorted[p]) ++p;  // the cell has a core
+        root = parent[c];
+        r = core_rank(core_bits, core_prefix, perm[p]);
+    }
+    unsigned pending = __ballot_sync(kFull, ok);
+    const int lane = threadIdx.x & 31;
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const int lroot = __shfl_sync(kFull, root, leader);
+        const bool mine = ok && root == lroot;
+        const int m = (int)__reduce_min_sync(kFull, mine ? (unsigned)r : (unsigned)kNoCluster);
+        if (lane == leader) atomicMin(comp_min + lroot, m);
+        pending &= ~__ballot_sync(kFull, mine);
+    }
+}
+
 // The one root of each cell's cores (parent flattened): -1 without cores, -2 when
 // they do not all share it.  One thread per point: the first core of a cell to
 // arrive installs its root, any core with another root marks the cell mixed; a
