@@ -82,6 +82,10 @@ constexpr size_t kSmallErrOff = 1536;        // int
 constexpr size_t kSmallStencilOff = 2048;    // int4[kMaxRows]: stencil rows of the current job
 constexpr size_t kSmallBytes = 4096;
 
+// Destination window of the input-order output scatters: 24M int32 (96 MB) stays
+// within the 126 MB L2, so outputs larger than that are written in several passes.
+constexpr int64_t kScatterWindow = int64_t(24) << 20;
+
 inline unsigned blocks_for(int64_t n, int threads = kBlock) {
     int64_t b = (n + threads - 1) / threads;
     return (unsigned)(b < 1 ? 1 : b);
@@ -628,9 +632,12 @@ void labels_phase(ndb_ctx *ctx) {
         ensure(ctx, ctx->ci_orig, (n + 1) * sizeof(int32_t));
         target = ctx->ci_orig.as<int32_t>();
     }
-    ++launch_counter(), output_ci_kernel<<<blocks_for(n), kBlock, 0, st>>>(
-        ctx->ci_sorted.as<int32_t>(), nv, n, ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(),
-        ctx->core_prefix.as<uint32_t>(), target, counters, nullptr, 0, nullptr);
+    const int64_t wci = target ? kScatterWindow : n;  // no output: one pass counts
+    for (int64_t lo = 0; lo < n; lo += wci)
+        ++launch_counter(), output_ci_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+            ctx->ci_sorted.as<int32_t>(), nv, n, ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(),
+            ctx->core_prefix.as<uint32_t>(), target, counters, nullptr, 0, nullptr, lo,
+            wci >= n ? INT64_MAX : lo + wci);
     ck(ctx, cudaGetLastError());
     cudaEventRecord(ctx->ev[4], st);
 }
@@ -716,8 +723,10 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
             ensure(ctx, ctx->nn_orig, (n + 1) * sizeof(int32_t));
             target = ctx->nn_orig.as<int32_t>();
         }
-        ++launch_counter(), scatter_nn_kernel<<<blocks_for(n), kBlock, 0, st>>>(
-            ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->ids0.as<int32_t>(), target, nullptr, 0);
+        for (int64_t lo = 0; lo < n; lo += kScatterWindow)
+            ++launch_counter(), scatter_nn_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+                ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->ids0.as<int32_t>(), target, nullptr, 0, lo,
+                n <= kScatterWindow ? INT64_MAX : lo + kScatterWindow);
         ck(ctx, cudaGetLastError());
         if (!(flags & NDB_FLAG_DEVICE_PTRS))
             ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));

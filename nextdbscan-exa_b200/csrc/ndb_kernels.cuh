@@ -668,13 +668,19 @@ __device__ __forceinline__ int32_t core_rank(const uint32_t *__restrict__ bits, 
 }
 
 // nn in input order (the caller's nn output)
+// Input-order outputs are random 4-byte writes.  When the output is much larger
+// than L2 the host runs the scatter in destination windows [win_lo, win_hi): each
+// pass streams the sorted arrays (evict-first loads) and writes only the points
+// whose destination falls in its window, so the partial-sector writes stay in L2.
 __global__ void scatter_nn_kernel(const int32_t *__restrict__ nn_sorted, int64_t nv, int64_t n,
                                   const int32_t *__restrict__ perm, int32_t *__restrict__ out,
-                                  const JobDev *__restrict__ jobs, int n_jobs) {
+                                  const JobDev *__restrict__ jobs, int n_jobs, int64_t win_lo = 0,
+                                  int64_t win_hi = INT64_MAX) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const int32_t o = perm[s];
-    const int32_t v = s < nv ? nn_sorted[s] : 0;
+    const int32_t o = __ldcs(perm + s);
+    if (o < win_lo || o >= win_hi) return;
+    const int32_t v = s < nv ? __ldcs(nn_sorted + s) : 0;
     if (jobs) {
         const JobDev &J = jobs[job_of_point(jobs, n_jobs, o)];
         if (J.nn_out) J.nn_out[o - J.off] = v;
@@ -1388,14 +1394,16 @@ __global__ void output_ci_kernel(const int32_t *__restrict__ ci_sorted, int64_t 
                                  const int32_t *__restrict__ perm, const uint32_t *__restrict__ core_bits,
                                  const uint32_t *__restrict__ core_prefix, int32_t *__restrict__ out,
                                  unsigned long long *__restrict__ counters, const JobDev *__restrict__ jobs,
-                                 int n_jobs, unsigned long long *__restrict__ job_counters) {
+                                 int n_jobs, unsigned long long *__restrict__ job_counters, int64_t win_lo = 0,
+                                 int64_t win_hi = INT64_MAX) {
+    // windows as in scatter_nn_kernel; every point is counted in its own window only
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned noise = 0, roots = 0;
-    if (s < n) {
-        const int32_t o = perm[s];
+    const int32_t o = s < n ? __ldcs(perm + s) : 0;
+    if (s < n && o >= win_lo && o < win_hi) {
         int32_t v;
         if (s < nv) {
-            v = ci_sorted[s];
+            v = __ldcs(ci_sorted + s);
         } else if (is_core_o(core_bits, o)) {
             v = core_rank(core_bits, core_prefix, o);
             roots = 1;

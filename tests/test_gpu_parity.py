@@ -223,3 +223,16 @@ def test_full_size_plain_3d_properties(ctx, pkg):
     assert (res_p.clusters, res_p.noise, res_p.core_count) == (res_f.clusters, res_f.noise, res_f.core_count)
     core_p = core[perm]
     np.testing.assert_array_equal(partition_key(ci_p[core_p]), partition_key(ci_f[perm][core_p]))
+
+
+def test_outputs_larger_than_l2_match_the_batched_path(ctx, pkg):
+    """Above 24M points the input-order outputs are scattered in destination
+    windows (several passes).  The batched entry point writes through its own
+    single-pass path; on one job both must agree exactly."""
+    w = pkg.synthetic.config1(n=30_000_000)
+    nn, ci, res = ctx.run(w.coords, w.eps, w.min_pts)
+    (nn_b, ci_b, res_b), = ctx.run_batched([(w.coords, w.eps, w.min_pts)])
+    np.testing.assert_array_equal(nn, nn_b)
+    np.testing.assert_array_equal(ci, ci_b)
+    assert res == res_b
+    assert res.noise == int(np.count_nonzero(ci == NO_CLUSTER))
