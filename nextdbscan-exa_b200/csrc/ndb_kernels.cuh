@@ -579,33 +579,53 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     // is still filling (count below list_cap): both warp-uniform, updated per chunk
     unsigned act = __ballot_sync(kFull, lane < cnt);
     unsigned lst = nbr_list && list_cap > 0 ? act : 0u;
+    // d >= 8: each lane holds two candidates per step (64 per warp), so an owned
+    // point is read from shared memory once per two pairs and the two distance sums
+    // (each in the reference's order) are independent chains for the scheduler
+    constexpr int CH = D >= 8 ? 2 : 1;
     int row = 0;  // this lane's stencil row: its candidate index only grows
-    for (int tb = 0; tb < total; tb += kWarp) {
-        const int t = tb + lane;
-        const int j = t < total ? row_next(rt, row, t) : -1;
-        float xj[D];
-        if (j >= 0) load_point<D>(xs, j, xj);
-        else fill_nan<D>(xj);  // NaN fails the predicate
+    for (int tb = 0; tb < total; tb += kWarp * CH) {
+        int j[CH];
+        float xj[CH][D];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int t = tb + c * kWarp + lane;
+            j[c] = t < total ? row_next(rt, row, t) : -1;
+            if (j[c] >= 0) load_point<D>(xs, j[c], xj[c]);
+            else fill_nan<D>(xj[c]);  // NaN fails the predicate
+        }
         int active = 0;
         for (unsigned it = act; it; it &= it - 1) {
             const int k = __ffs(it) - 1;
             float xi[D];
             load_point_smem<D>(si + k * P, xi);
-            const bool hit = in_range<D>(xi, xj, e2);
-            const unsigned m = __ballot_sync(kFull, hit);
+            bool hit[CH];
+            unsigned m[CH];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) hit[c] = in_range<D>(xi, xj[c], e2);
+#pragma unroll
+            for (int c = 0; c < CH; ++c) m[c] = __ballot_sync(kFull, hit[c]);
             // the first list_cap neighbours of each point; complete for every point
             // whose count stays below min_pts (list_cap = min_pts - 1)
             if ((lst >> k) & 1u) {
-                const int slot = __shfl_sync(kFull, mycnt, k) + __popc(m & lanemask_lt());
-                if (hit && slot < list_cap) {
-                    if (smem_list) sl[k * kSmemListCap + slot] = j;
-                    else nbr_list[(int64_t)(p0 + k) * list_stride + slot] = j;
+                int base = __shfl_sync(kFull, mycnt, k);
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    const int slot = base + __popc(m[c] & lanemask_lt());
+                    if (hit[c] && slot < list_cap) {
+                        if (smem_list) sl[k * kSmemListCap + slot] = j[c];
+                        else nbr_list[(int64_t)(p0 + k) * list_stride + slot] = j[c];
+                    }
+                    base += __popc(m[c]);
                 }
             }
-            if (lane == k) mycnt += __popc(m);
+            int got = 0;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) got += __popc(m[c]);
+            if (lane == k) mycnt += got;
             ++active;
         }
-        pairs += (unsigned long long)active * (unsigned long long)min(kWarp, total - tb);
+        pairs += (unsigned long long)active * (unsigned long long)min(kWarp * CH, total - tb);
         if (lst) lst &= __ballot_sync(kFull, mycnt < list_cap);
         if (EARLY) {
             act = __ballot_sync(kFull, lane < cnt && mycnt < min_pts);
