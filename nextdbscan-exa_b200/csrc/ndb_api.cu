@@ -1448,11 +1448,6 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
             return;
         }
     }
-    if (getenv("NDB_DEBUG")) {
-        for (int m = 0; m < nj; ++m)
-            fprintf(stderr, "ndb batch d=%d job %d: off=%lld n=%lld invalid=%llu key_base=%llu k=%d\n", D, members[m],
-                    (long long)bp.jd[m].off, (long long)bp.jd[m].n, h_inval[m], bp.jd[m].key_base, bp.jd[m].g.k);
-    }
     // outputs: device pointers go straight to the kernels; host ones through staging
     if (flags & NDB_FLAG_DEVICE_PTRS) {
         for (int m = 0; m < nj; ++m) {
