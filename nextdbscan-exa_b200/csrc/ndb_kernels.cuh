@@ -890,21 +890,37 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
     int rootA = 0;
     if (lane == 0) rootA = uf_find(parent, A, err);
     rootA = __shfl_sync(kFull, rootA, 0);
+    // Candidate cells, four per lane per step so that their load chains overlap.  The
+    // root test uses an ancestor two hops up (parents were flattened before this
+    // kernel, so usually the root): equal to A's root means already joined; an
+    // ancestor that is not yet the root only costs a needless probe below.
+    constexpr int U = 4;
     int nb = 0;
-    for (int tb = 0; tb < total; tb += kWarp) {
-        const int t = tb + lane;
-        bool ok = false;
-        int B = 0;
-        if (t < total) {
-            B = row_lookup(rt, n_rows, t);
-            ok = cell_has_core[B] && uf_find(parent, B, err) != rootA;
+    for (int tb = 0; tb < total; tb += kWarp * U) {
+        int B[U], p[U];
+        bool hc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int t = tb + u * kWarp + lane;
+            B[u] = t < total ? row_lookup(rt, n_rows, t) : -1;
         }
-        const unsigned mask = __ballot_sync(kFull, ok);
-        if (ok) {
-            const int slot = nb + __popc(mask & lanemask_lt());
-            if (slot < kMaxCandCells) sb[slot] = B;
+#pragma unroll
+        for (int u = 0; u < U; ++u) hc[u] = B[u] >= 0 && cell_has_core[B[u]];
+#pragma unroll
+        for (int u = 0; u < U; ++u) p[u] = hc[u] ? __ldcg(parent + B[u]) : -1;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (hc[u] && p[u] != B[u]) p[u] = __ldcg(parent + p[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool ok = hc[u] && p[u] != rootA;
+            const unsigned mask = __ballot_sync(kFull, ok);
+            if (ok) {
+                const int slot = nb + __popc(mask & lanemask_lt());
+                if (slot < kMaxCandCells) sb[slot] = B[u];
+            }
+            nb += __popc(mask);
         }
-        nb += __popc(mask);
     }
     __syncwarp();
     nb = min(nb, kMaxCandCells);
