@@ -1053,7 +1053,31 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) union_points_kernel(
     if (total < 0) total = gather_rows<false>(nbr + (int64_t)A * n_rows, n_rows, cell_start, 0, rt, lane);
     unsigned long long pairs = 0;
     int cur = 0;  // this lane's stencil row
+    // the next step's candidate, its core flag and its parent are loaded one step
+    // ahead (independent loads), so their latency overlaps this step's root refresh
+    // and tests; a parent read early is still an ancestor, so a stale one can only
+    // cost an extra predicate, never a missed union
+    int jn = lane < total ? row_next(rt, cur, lane) : -1;
+    bool cn = false;
+    int pn = -1;
+    if (jn >= 0) {
+        cn = core_sorted[jn] != 0;
+        pn = __ldcg(parent + jn);
+    }
     for (int tb = 0; tb < total; tb += kWarp) {
+        const int j = jn;
+        bool valid = j > p0 && cn;
+        int pj = pn;
+        {
+            const int t = tb + kWarp + lane;
+            jn = t < total ? row_next(rt, cur, t) : -1;
+            cn = false;
+            pn = -1;
+            if (jn >= 0) {
+                cn = core_sorted[jn] != 0;
+                pn = __ldcg(parent + jn);
+            }
+        }
         // roots of the item's cores, refreshed every chunk so that candidates already
         // joined to them are skipped before the predicate
         int myroot = lane < nc ? uf_find(parent, sidx[lane], err) : -1;
@@ -1062,15 +1086,9 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) union_points_kernel(
         const int root0 = __shfl_sync(kFull, myroot, 0);
         const bool uniform = __all_sync(kFull, lane >= nc || myroot == root0);
         __syncwarp();
-        const int t = tb + lane;
-        int j = -1;
-        if (t < total) j = row_next(rt, cur, t);
-        bool valid = j > p0 && core_sorted[j];
         float xj[D];
-        int pj = -1;
         if (valid) {
-            pj = __ldcg(parent + j);
-            pj = __ldcg(parent + pj);  // two hops: an ancestor of j, usually its root
+            pj = __ldcg(parent + pj);  // second hop: an ancestor of j, usually its root
             if (uniform && pj == root0) valid = false;  // joined to every core of the item already
         }
         if (!__any_sync(kFull, valid)) continue;
