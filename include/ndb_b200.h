@@ -179,6 +179,20 @@ ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t n_jobs, uin
  * (data_process.cpp:79-88).  Host buffer of at least core_count entries. */
 ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capacity);
 
+/* Caps the device memory the context may hold, in bytes (0 = no cap, the default).
+ * A run whose buffers would grow past the cap fails with NDB_ERR_OUT_OF_MEMORY before
+ * it allocates anything, and the context stays usable for the next run.  A cap below
+ * what the context holds now releases all its buffers (after the context's stream
+ * drains); a pending ndb_b200_assign_labels then returns NDB_ERR_NO_STATE.  Lets a
+ * caller share one GPU with other work at a known footprint, and injects allocation
+ * failures in tests.  No counterpart in the reference, which only tracks its host
+ * footprint (allocated_bytes, data_process.h:54,63,75,79-85) and exits on failure. */
+ndb_status ndb_b200_set_memory_limit(ndb_ctx *ctx, int64_t max_bytes);
+
+/* Device bytes the context holds now (its buffers grow to the largest job run and
+ * are kept until ndb_b200_destroy or a lower memory cap). */
+ndb_status ndb_b200_device_bytes(ndb_ctx *ctx, int64_t *bytes);
+
 /* Counters and phase times of the last run. */
 ndb_status ndb_b200_get_stats(ndb_ctx *ctx, ndb_stats *stats);
 
@@ -198,7 +212,7 @@ const char *ndb_b200_version(void);
  * reserves its GPU memory once at start-up and forbids cudaMalloc later, or a host
  * program that only lends out buffers it owns.  No counterpart in the reference.
  * Every scratch buffer comes from one fixed device array inside the library (about
- * 12 MiB, held by every GPU that loads the library until the process exits); the
+ * 16 MiB, held by every GPU that loads the library until the process exits); the
  * call makes no cudaMalloc or cudaFree.  coords, nn_out and cluster_index_out are
  * device pointers on the current device (outputs may be NULL); the work runs on
  * cuda_stream (NULL: the legacy default stream) and is complete when the call

@@ -196,6 +196,18 @@ class Context:
         lib.check(st, "ndb_b200_cluster_label", self._h)
         return out
 
+    def set_memory_limit(self, max_bytes: int) -> None:
+        """Caps the context's device footprint (0 = no cap); a run past it raises
+        NdbError(NDB_ERR_OUT_OF_MEMORY) and leaves the context usable."""
+        lib.check(self._lib.ndb_b200_set_memory_limit(self._h, int(max_bytes)), "ndb_b200_set_memory_limit",
+                  self._h)
+
+    def device_bytes(self) -> int:
+        """Device memory the context holds now."""
+        out = ctypes.c_int64()
+        lib.check(self._lib.ndb_b200_device_bytes(self._h, ctypes.byref(out)), "ndb_b200_device_bytes", self._h)
+        return out.value
+
     def stats(self) -> dict:
         s = lib.NdbStats()
         lib.check(self._lib.ndb_b200_get_stats(self._h, ctypes.byref(s)), "ndb_b200_get_stats", self._h)

@@ -44,6 +44,25 @@ struct ndb_ctx {
     DevBuf jobs_dev, batch_bbox, cell_job, job_counters;
     // items split between the tensor-core count (full items) and the exact one
     DevBuf items_split;
+    // largest device footprint the context may hold (bytes); 0 = no cap
+    size_t mem_limit = 0;
+
+    template <typename F>
+    void for_each_buf(F f) {
+        DevBuf *bufs[] = {&coords,      &keys0,       &keys1,       &ids0,        &ids1,        &flags,
+                          &pos,         &pcell,       &xs,          &nn_sorted,   &nn_orig,     &core_sorted,
+                          &core_bits,   &core_prefix, &ci_sorted,   &ci_orig,     &labels,      &cell_start,
+                          &cell_key,    &nbr,         &item_cnt,    &items,       &cell_has_core, &cell_cid,
+                          &parent,      &comp_min,    &sort_hist,   &scan_scratch, &small,      &hash_keys,
+                          &hash_vals,   &nbr_list,    &jobs_dev,    &batch_bbox,  &cell_job,    &job_counters,
+                          &items_split};
+        for (DevBuf *b : bufs) f(*b);
+    }
+    size_t held_bytes() {
+        size_t total = 0;
+        for_each_buf([&](DevBuf &b) { total += b.bytes; });
+        return total;
+    }
 
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     // kernel-level events: sort, count, union, border (begin, end)
@@ -101,7 +120,18 @@ inline void ck(ndb_ctx *ctx, cudaError_t e) {
     throw Fail{e == cudaErrorMemoryAllocation ? NDB_ERR_OUT_OF_MEMORY : NDB_ERR_CUDA};
 }
 
-inline void ensure(ndb_ctx *ctx, DevBuf &b, size_t bytes) { ck(ctx, b.ensure(bytes < 16 ? 16 : bytes)); }
+// Grows b to at least `bytes`, refusing (as an allocation failure, before any
+// cudaMalloc) when the context's footprint would pass its memory cap.
+inline cudaError_t grow(ndb_ctx *ctx, DevBuf &b, size_t bytes) {
+    if (bytes < 16) bytes = 16;
+    if (ctx->mem_limit && bytes > b.bytes) {
+        const size_t rounded = (bytes + 4095) & ~size_t(4095);
+        if (ctx->held_bytes() - b.bytes + rounded > ctx->mem_limit) return cudaErrorMemoryAllocation;
+    }
+    return b.ensure(bytes);
+}
+
+inline void ensure(ndb_ctx *ctx, DevBuf &b, size_t bytes) { ck(ctx, grow(ctx, b, bytes)); }
 
 template <typename T>
 T *small_at(ndb_ctx *ctx, size_t off) {
@@ -881,21 +911,33 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
     if (!ctx) return NDB_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf *bufs[] = {&ctx->coords,      &ctx->keys0,     &ctx->keys1,      &ctx->ids0,        &ctx->ids1,
-                      &ctx->flags,       &ctx->pos,       &ctx->pcell,      &ctx->xs,          &ctx->nn_sorted,
-                      &ctx->nn_orig,     &ctx->core_sorted, &ctx->core_bits, &ctx->core_prefix, &ctx->ci_sorted,
-                      &ctx->ci_orig,     &ctx->labels,    &ctx->cell_start, &ctx->cell_key,    &ctx->nbr,
-                      &ctx->item_cnt,    &ctx->items,     &ctx->cell_has_core, &ctx->cell_cid, &ctx->parent,
-                      &ctx->comp_min,    &ctx->sort_hist, &ctx->scan_scratch, &ctx->small,
-                      &ctx->hash_keys,   &ctx->hash_vals, &ctx->nbr_list, &ctx->jobs_dev,
-                      &ctx->batch_bbox,  &ctx->cell_job,  &ctx->job_counters, &ctx->items_split};
-    for (DevBuf *b : bufs) b->release();
+    ctx->for_each_buf([](DevBuf &b) { b.release(); });
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : ctx->kev)
         if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_set_memory_limit(ndb_ctx *ctx, int64_t max_bytes) {
+    if (!ctx || max_bytes < 0) return NDB_ERR_INVALID_ARGUMENT;
+    ctx->mem_limit = (size_t)max_bytes;
+    if (ctx->mem_limit && ctx->held_bytes() > ctx->mem_limit) {
+        // drop every buffer; the next run allocates what it needs under the new cap
+        cudaSetDevice(ctx->device);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return NDB_ERR_CUDA;
+        ctx->for_each_buf([](DevBuf &b) { b.release(); });
+        ctx->have_state = false;
+        ctx->have_labels = false;
+    }
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_device_bytes(ndb_ctx *ctx, int64_t *bytes) {
+    if (!ctx || !bytes) return NDB_ERR_INVALID_ARGUMENT;
+    *bytes = (int64_t)ctx->held_bytes();
     return NDB_OK;
 }
 
@@ -970,7 +1012,8 @@ ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capa
     if (!ctx->have_labels) return NDB_ERR_NO_STATE;
     if (capacity < ctx->n_cores || (ctx->n_cores > 0 && !label_out)) return NDB_ERR_INVALID_ARGUMENT;
     if (ctx->n_cores == 0) return NDB_OK;
-    if (ctx->labels.ensure((size_t)(ctx->n_cores + 1) * sizeof(int32_t)) != cudaSuccess) return NDB_ERR_OUT_OF_MEMORY;
+    if (grow(ctx, ctx->labels, (size_t)(ctx->n_cores + 1) * sizeof(int32_t)) != cudaSuccess)
+        return NDB_ERR_OUT_OF_MEMORY;
     ++launch_counter(), labels_kernel<<<blocks_for(ctx->n), kBlock, 0, ctx->stream>>>(
         ctx->ci_sorted.as<int32_t>(), ctx->nv, ctx->n, ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(),
         ctx->core_prefix.as<uint32_t>(), ctx->labels.as<int32_t>());
@@ -1492,7 +1535,7 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     ctx->have_labels = false;
     ctx->stats = ndb_stats{};
     launch_counter() = 0;
-    if (ctx->small.ensure(kSmallBytes) != cudaSuccess) return NDB_ERR_OUT_OF_MEMORY;
+    if (grow(ctx, ctx->small, kSmallBytes) != cudaSuccess) return NDB_ERR_OUT_OF_MEMORY;
     if (cudaMemsetAsync(ctx->small.ptr, 0, kSmallBytes, ctx->stream) != cudaSuccess) return NDB_ERR_CUDA;
     ndb_status first = NDB_OK;
     // validate, and group by dimensionality
@@ -1621,7 +1664,7 @@ enum NaBuf {
     NA_KEYS0, NA_KEYS1, NA_IDS0, NA_IDS1, NA_FLAGS, NA_POS, NA_PCELL, NA_XS, NA_NN_SORTED, NA_NN_ORIG,
     NA_CORE_SORTED, NA_CORE_BITS, NA_CORE_PREFIX, NA_CI_SORTED, NA_CI_ORIG, NA_LABELS, NA_CELL_START, NA_CELL_KEY,
     NA_NBR, NA_ITEM_CNT, NA_ITEMS, NA_CELL_HAS_CORE, NA_CELL_CID, NA_PARENT, NA_COMP_MIN, NA_SORT_HIST,
-    NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_NBR_LIST, NA_COUNT
+    NA_SCAN, NA_SMALL, NA_HASH_KEYS, NA_HASH_VALS, NA_NBR_LIST, NA_ITEMS_SPLIT, NA_COUNT
 };
 
 constexpr size_t na_cap(int b) {
@@ -1638,6 +1681,7 @@ constexpr size_t na_cap(int b) {
          : b == NA_HASH_KEYS ? 8 * 4 * kNaN
          : b == NA_HASH_VALS ? 4 * 4 * kNaN
          : b == NA_NBR_LIST ? 4 * 16 * kNaN
+         : b == NA_ITEMS_SPLIT ? 16 * (kNaN + 1)  // both item lists of the tensor-core count (items <= n)
          : 4 * (kNaN + 1);
 }
 
@@ -1661,7 +1705,7 @@ DevBuf *na_buf(ndb_ctx &c, int b) {
                               &c.labels,      &c.cell_start, &c.cell_key, &c.nbr,          &c.item_cnt,
                               &c.items,       &c.cell_has_core, &c.cell_cid, &c.parent,    &c.comp_min,
                               &c.sort_hist,   &c.scan_scratch, &c.small,     &c.hash_keys, &c.hash_vals,
-                              &c.nbr_list};
+                              &c.nbr_list,    &c.items_split};
     return bufs[b];
 }
 
@@ -1720,6 +1764,9 @@ extern "C" ndb_status ndb_b200_run_noalloc(const float *coords, int64_t n, int32
         s.ready = true;
     }
     na_carve(s);
+    // cap the footprint at the slices themselves: a request that would outgrow its
+    // slice is refused before any cudaFree/cudaMalloc instead of reallocating
+    s.ctx.mem_limit = s.ctx.held_bytes();
     s.ctx.list_budget = na_cap(NA_NBR_LIST) - 4;  // lists only where they fit the slice
     s.ctx.own_stream = nullptr;
     s.ctx.stream = static_cast<cudaStream_t>(cuda_stream);

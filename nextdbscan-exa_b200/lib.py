@@ -46,6 +46,8 @@ EXPORTED = (
     "ndb_b200_run_batched",
     "ndb_b200_cluster_label",
     "ndb_b200_get_stats",
+    "ndb_b200_set_memory_limit",
+    "ndb_b200_device_bytes",
     "ndb_b200_strerror",
     "ndb_b200_last_cuda_error",
     "ndb_b200_version",
@@ -144,6 +146,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
                                              ctypes.c_uint32]
         lib.ndb_b200_cluster_label.argtypes = [ctypes.c_void_p, i32p, ctypes.c_int64]
         lib.ndb_b200_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbStats)]
+        lib.ndb_b200_set_memory_limit.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+        lib.ndb_b200_device_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
         lib.ndb_b200_strerror.argtypes = [ctypes.c_int]
         lib.ndb_b200_strerror.restype = ctypes.c_char_p
         lib.ndb_b200_last_cuda_error.argtypes = [ctypes.c_void_p]
@@ -151,7 +155,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_version.restype = ctypes.c_char_p
         for name in ("ndb_b200_create", "ndb_b200_destroy", "ndb_b200_set_stream", "ndb_b200_classify",
                      "ndb_b200_assign_labels", "ndb_b200_run", "ndb_b200_run_batched", "ndb_b200_cluster_label",
-                     "ndb_b200_get_stats"):
+                     "ndb_b200_get_stats", "ndb_b200_set_memory_limit", "ndb_b200_device_bytes"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib

@@ -63,6 +63,8 @@ def test_status_codes_without_gpu():
     lib = pkg.lib.load()
     h = ctypes.c_void_p()
     assert lib.ndb_b200_create(None, 0) == 1  # null out-pointer
+    assert lib.ndb_b200_set_memory_limit(None, 0) == 1
+    assert lib.ndb_b200_device_bytes(None, None) == 1
     if cuda_available():
         pytest.skip("a GPU is present; the no-device path is not reachable")
     assert lib.ndb_b200_create(ctypes.byref(h), 0) == 7  # NDB_ERR_NO_DEVICE
