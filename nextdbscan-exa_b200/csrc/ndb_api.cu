@@ -23,6 +23,13 @@ struct ndb_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    // ndb_b200_run with host outputs: the counts go back to the host on this stream
+    // while the label phase runs on `stream`
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_nn = nullptr;
+    bool in_run = false;     // classify is the first half of ndb_b200_run
+    bool nn_pending = false; // a count copy on copy_stream not yet waited for
+    bool stats_pending = false; // classify's counters are read by the label phase
     std::string last_cuda_error;
 
     // inputs / per-point arrays
@@ -687,6 +694,26 @@ bool is_device_ptr(const void *p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Counters and times of phase 1, once its work on the context's stream is done.
+template <int D>
+void classify_stats(ndb_ctx *ctx) {
+    unsigned long long h_counters[8];
+    uint32_t h_tc_items = 0;
+    ck(ctx, cudaMemcpyAsync(h_counters, small_at<unsigned long long>(ctx, kSmallCountersOff), sizeof(h_counters),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    ck(ctx, cudaMemcpyAsync(&h_tc_items, small_at<uint32_t>(ctx, kSmallScalarOff) + 4, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    ck(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->stats.tensor_items = ctx->tc_count ? h_tc_items : 0;
+    ctx->stats.count_pairs = (int64_t)h_counters[2];
+    ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
+    ctx->stats.band_pairs = (int64_t)h_counters[5];
+    ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
+    ctx->stats.ms_count = elapsed(ctx->ev[1], ctx->ev[2]);
+    ctx->stats.ms_sort_kernels = elapsed(ctx->kev[0], ctx->kev[1]);
+    ctx->stats.ms_count_kernel = elapsed(ctx->kev[2], ctx->kev[3]);
+}
+
 template <int D>
 ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps, int32_t min_pts, uint32_t flags,
                          int32_t *nn_out) {
@@ -699,6 +726,7 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->min_pts = min_pts;
     ctx->flags_run = flags;
     ctx->stats = ndb_stats{};
+    ctx->stats_pending = false;
     launch_counter() = 0;
     ensure(ctx, ctx->small, kSmallBytes);
     ck(ctx, cudaMemsetAsync(ctx->small.ptr, 0, kSmallBytes, st));
@@ -758,17 +786,19 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
                 ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->ids0.as<int32_t>(), target, nullptr, 0, lo,
                 n <= kScatterWindow ? INT64_MAX : lo + kScatterWindow);
         ck(ctx, cudaGetLastError());
-        if (!(flags & NDB_FLAG_DEVICE_PTRS))
-            ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        if (!(flags & NDB_FLAG_DEVICE_PTRS)) {
+            if (ctx->in_run && ctx->copy_stream) {
+                // nothing later in the job writes nn_orig: the copy overlaps the label phase
+                ck(ctx, cudaEventRecord(ctx->ev_nn, st));
+                ck(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_nn, 0));
+                ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                        ctx->copy_stream));
+                ctx->nn_pending = true;
+            } else {
+                ck(ctx, cudaMemcpyAsync(nn_out, ctx->nn_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            }
+        }
     }
-    unsigned long long h_counters[8];
-    uint32_t h_tc_items = 0;
-    ck(ctx, cudaMemcpyAsync(h_counters, small_at<unsigned long long>(ctx, kSmallCountersOff), sizeof(h_counters),
-                            cudaMemcpyDeviceToHost, st));
-    ck(ctx, cudaMemcpyAsync(&h_tc_items, small_at<uint32_t>(ctx, kSmallScalarOff) + 4, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, st));
-    ck(ctx, cudaStreamSynchronize(st));
-    ctx->stats.tensor_items = ctx->tc_count ? h_tc_items : 0;
     ctx->stats.n_valid = ctx->nv;
     ctx->stats.n_cells = ctx->n_cells;
     ctx->stats.n_tiles = ctx->n_items;
@@ -776,15 +806,17 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->stats.stencil_rows = pl.st.n_rows;
     ctx->stats.same_cell_linked = ctx->cell_units;
     ctx->stats.key_bits = pl.key_bits;
-    ctx->stats.count_pairs = (int64_t)h_counters[2];
-    ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
-    ctx->stats.band_pairs = (int64_t)h_counters[5];
     ctx->stats.tensor_filter = ctx->tc_count ? 1 : 0;
-    ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
-    ctx->stats.ms_count = elapsed(ctx->ev[1], ctx->ev[2]);
-    ctx->stats.ms_sort_kernels = elapsed(ctx->kev[0], ctx->kev[1]);
-    ctx->stats.ms_count_kernel = elapsed(ctx->kev[2], ctx->kev[3]);
     ctx->have_state = true;
+    if (ctx->in_run) {
+        // ndb_b200_run goes on with the label phase, which reads these counters with
+        // its own: no host round trip between the phases, and no host read queued
+        // behind the count copy on the copy engine
+        ctx->stats_pending = true;
+        return NDB_OK;
+    }
+    ck(ctx, cudaStreamSynchronize(st));
+    classify_stats<D>(ctx);
     return NDB_OK;
 }
 
@@ -806,6 +838,19 @@ ndb_status labels_impl(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
                             st));
     ck(ctx, cudaMemcpyAsync(&h_err, small_at<int>(ctx, kSmallErrOff), sizeof(int), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaStreamSynchronize(st));
+    if (ctx->stats_pending) {
+        // classify_stats without its own copies: the label phase leaves counters 2 and 5
+        // and scalar 4 as phase 1 wrote them
+        ctx->stats_pending = false;
+        ctx->stats.tensor_items = ctx->tc_count ? h_scal[4] : 0;
+        ctx->stats.count_pairs = (int64_t)h_counters[2];
+        ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
+        ctx->stats.band_pairs = (int64_t)h_counters[5];
+        ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
+        ctx->stats.ms_count = elapsed(ctx->ev[1], ctx->ev[2]);
+        ctx->stats.ms_sort_kernels = elapsed(ctx->kev[0], ctx->kev[1]);
+        ctx->stats.ms_count_kernel = elapsed(ctx->kev[2], ctx->kev[3]);
+    }
     if (h_err) return NDB_ERR_DEVICE_LIMIT;
     ctx->n_cores = h_scal[2];
     ctx->result.clusters = (int32_t)h_counters[0];
@@ -891,6 +936,11 @@ ndb_status ndb_b200_create(ndb_ctx **out, int32_t device) {
         return NDB_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
+    if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_nn, cudaEventDisableTiming) != cudaSuccess) {
+        ndb_b200_destroy(ctx);
+        return NDB_ERR_CUDA;
+    }
     for (auto &e : ctx->ev) {
         if (cudaEventCreate(&e) != cudaSuccess) {
             delete ctx;
@@ -911,11 +961,14 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
     if (!ctx) return NDB_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     ctx->for_each_buf([](DevBuf &b) { b.release(); });
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : ctx->kev)
         if (e) cudaEventDestroy(e);
+    if (ctx->ev_nn) cudaEventDestroy(ctx->ev_nn);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return NDB_OK;
@@ -1001,9 +1054,18 @@ ndb_status ndb_b200_assign_labels(ndb_ctx *ctx, int32_t *cluster_index_out, ndb_
 
 ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
                         uint32_t flags, int32_t *nn_out, int32_t *cluster_index_out, ndb_result *result) {
+    if (!ctx) return NDB_ERR_INVALID_ARGUMENT;
+    ctx->in_run = true;
     ndb_status s = ndb_b200_classify(ctx, coords, n, d, eps, min_pts, flags, nn_out);
-    if (s != NDB_OK) return s;
-    return ndb_b200_assign_labels(ctx, cluster_index_out, result);
+    ctx->in_run = false;
+    if (s == NDB_OK) s = ndb_b200_assign_labels(ctx, cluster_index_out, result);
+    if (ctx->nn_pending) {
+        // the counts are in the caller's buffer only once their copy is done
+        ctx->nn_pending = false;
+        cudaSetDevice(ctx->device);
+        if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && s == NDB_OK) s = NDB_ERR_CUDA;
+    }
+    return s;
 }
 
 ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capacity) {

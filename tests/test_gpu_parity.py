@@ -146,6 +146,31 @@ def test_device_pointer_path(ctx, pkg):
     assert meta_of(res) == list(g["meta"])
 
 
+def test_pinned_host_buffers(ctx, pkg):
+    """Pinned host outputs: the count copy runs on its own stream, overlapping the
+    label phase; the call returns only when both outputs are complete."""
+    import torch
+    w = pkg.synthetic.config2(n=200_000)
+    n, d = w.coords.shape
+    hx = torch.from_numpy(w.coords).pin_memory()
+    nn_o, ci_o, meta = oracle.grid(w.coords, w.eps, w.min_pts)
+    for rep in range(3):
+        for full in (True, False):
+            hnn = torch.full((n,), -7, dtype=torch.int32).pin_memory()
+            hci = torch.full((n,), -7, dtype=torch.int32).pin_memory()
+            res = ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
+                               full_count=full)
+            nn, ci = hnn.numpy(), hci.numpy()
+            np.testing.assert_array_equal(ci, ci_o)
+            if full:
+                np.testing.assert_array_equal(nn, nn_o)
+            else:
+                below = nn_o < w.min_pts
+                np.testing.assert_array_equal(nn[below], nn_o[below])
+                assert (nn[~below] >= w.min_pts).all()
+            assert (res.clusters, res.noise, res.core_count) == (meta["clusters"], meta["noise"], meta["cores"])
+
+
 def test_error_statuses(ctx, pkg):
     x = np.zeros((10, 17), np.float32)
     with pytest.raises(pkg.lib.NdbError, match="UNSUPPORTED_DIM"):
