@@ -216,7 +216,9 @@ const char *ndb_b200_version(void);
  * call makes no cudaMalloc or cudaFree.  coords, nn_out and cluster_index_out are
  * device pointers on the current device (outputs may be NULL); the work runs on
  * cuda_stream (NULL: the legacy default stream) and is complete when the call
- * returns.  n above NDB_NOALLOC_MAX_POINTS returns NDB_ERR_TOO_MANY_POINTS.
+ * returns.  n above NDB_NOALLOC_MAX_POINTS returns NDB_ERR_TOO_MANY_POINTS; a
+ * buffer request beyond its slice of the array returns NDB_ERR_OUT_OF_MEMORY (the
+ * slices are sized for the largest request of any job within the limit).
  * The first call on a device does the set-up (it looks up the array's device
  * address and creates the shared state's timing events), so make it before any
  * stream capture.  Calls share the array: they are serialised per device, and GPU
