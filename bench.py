@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--jobs", type=int, default=4096, help="jobs of the batched configuration 4")
     ap.add_argument("--count-kernel", choices=["auto", "exact", "tensor"], default="auto",
                     help="neighbour-count kernel for d >= 8: picked per item (auto), exact FP32 only, or tensor filter")
+    ap.add_argument("--autotune", action="store_true",
+                    help="d >= 8: pick the count-kernel thresholds on the workload before timing")
     ap.add_argument("--no-plain", action="store_true", help="configuration 4: skip the one-call-per-job form")
     ap.add_argument("--dims", type=str, default=None,
                     help="configuration 4: keep only the jobs of these dimensionalities (comma list)")
@@ -291,6 +293,13 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     ck_kw = {"exact": {"exact_count": True}, "tensor": {"tensor_filter": True}}.get(args.count_kernel, {})
+    tuning = None
+    if args.autotune and d >= 8 and not ck_kw:
+        # untimed: the count-kernel thresholds picked on this workload, then left on the context
+        r = pkg.autotune.tune_count(ctx, w.coords, w.eps, w.min_pts, full_count=full)
+        tuning = {"best": r["best"],
+                  "count_kernel_ms": {f"min_dim={c['tc_min_dim']},min_item={c['tc_min_item']}":
+                                      round(c["ms_count_kernel"], 4) for c in r["table"]}}
 
     def step():
         return ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(), full_count=full,
@@ -406,7 +415,7 @@ def run_ours(args):
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk_sum,
-            "gpu_launches": launches * args.steps, "count_forms": forms or None,
+            "gpu_launches": launches * args.steps, "count_forms": forms or None, "tuning": tuning,
             "tensor_filter": {"used": bool(s0["tensor_filter"]), "items": s0["tensor_items"], "of_items": s0["n_tiles"],
                               "band_pairs": s0["band_pairs"]},
             "result": {"clusters": res.clusters, "noise": res.noise, "core_count": res.core_count},

@@ -189,6 +189,30 @@ ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capa
  * footprint (allocated_bytes, data_process.h:54,63,75,79-85) and exits on failure. */
 ndb_status ndb_b200_set_memory_limit(ndb_ctx *ctx, int64_t max_bytes);
 
+/* Count-kernel thresholds of a context, picked by measurement (the autotuner of
+ * the Python package times the candidates on a sample of the caller's data).  They
+ * choose which kernel counts neighbours; results never depend on them.  0 = the
+ * library's default.  No counterpart in the reference, whose count has one form.
+ *   tc_min_dim   smallest d at which the count may run on the tensor-core filter
+ *                (clamped to >= 8).  Default: 8 with NDB_FLAG_FULL_COUNT, 12 with the
+ *                early exit (or the NDB_TC_MIN_DIM environment variable); a value
+ *                above 16 keeps every count on the exact kernel.
+ *   tc_min_item  smallest item (points of one cell, up to 32) the tensor-core filter
+ *                takes; smaller items go to the exact kernel.  Default 16 (or
+ *                NDB_TC_MIN_ITEM); above 32 sends every item to the exact kernel.
+ * NDB_FLAG_EXACT_COUNT and NDB_FLAG_TENSOR_FILTER on a call override both. */
+typedef struct ndb_tuning {
+    int32_t tc_min_dim;
+    int32_t tc_min_item;
+} ndb_tuning;
+
+/* Sets the context's thresholds (NULL: back to the defaults); negative values are
+ * NDB_ERR_INVALID_ARGUMENT. */
+ndb_status ndb_b200_set_tuning(ndb_ctx *ctx, const ndb_tuning *tuning);
+
+/* The context's thresholds as set (0 where the default applies). */
+ndb_status ndb_b200_get_tuning(ndb_ctx *ctx, ndb_tuning *tuning);
+
 /* Device bytes the context holds now (its buffers grow to the largest job run and
  * are kept until ndb_b200_destroy or a lower memory cap). */
 ndb_status ndb_b200_device_bytes(ndb_ctx *ctx, int64_t *bytes);

@@ -22,10 +22,10 @@ from typing import NamedTuple
 
 import numpy as np
 
-from . import inputs, lib, synthetic
+from . import autotune, inputs, lib, synthetic
 
 NO_CLUSTER = lib.NDB_NO_CLUSTER
-__all__ = ["Context", "Result", "data_process", "start", "inputs", "synthetic", "lib", "NO_CLUSTER"]
+__all__ = ["Context", "Result", "data_process", "start", "autotune", "inputs", "synthetic", "lib", "NO_CLUSTER"]
 
 
 class Result(NamedTuple):
@@ -201,6 +201,20 @@ class Context:
         NdbError(NDB_ERR_OUT_OF_MEMORY) and leaves the context usable."""
         lib.check(self._lib.ndb_b200_set_memory_limit(self._h, int(max_bytes)), "ndb_b200_set_memory_limit",
                   self._h)
+
+    def set_tuning(self, tc_min_dim: int = 0, tc_min_item: int = 0) -> None:
+        """Count-kernel thresholds of this context (0 = library default); see
+        ndb_tuning in include/ndb_b200.h.  Results never depend on them."""
+        t = lib.NdbTuning(int(tc_min_dim), int(tc_min_item))
+        lib.check(self._lib.ndb_b200_set_tuning(self._h, ctypes.byref(t)), "ndb_b200_set_tuning", self._h)
+
+    def reset_tuning(self) -> None:
+        lib.check(self._lib.ndb_b200_set_tuning(self._h, None), "ndb_b200_set_tuning", self._h)
+
+    def tuning(self) -> dict:
+        t = lib.NdbTuning()
+        lib.check(self._lib.ndb_b200_get_tuning(self._h, ctypes.byref(t)), "ndb_b200_get_tuning", self._h)
+        return {"tc_min_dim": t.tc_min_dim, "tc_min_item": t.tc_min_item}
 
     def device_bytes(self) -> int:
         """Device memory the context holds now."""

@@ -53,6 +53,8 @@ struct ndb_ctx {
     DevBuf items_split;
     // largest device footprint the context may hold (bytes); 0 = no cap
     size_t mem_limit = 0;
+    // count-kernel thresholds set by ndb_b200_set_tuning (0: the library's defaults)
+    ndb_tuning tuning{0, 0};
 
     template <typename F>
     void for_each_buf(F f) {
@@ -407,16 +409,25 @@ void count_phase(ndb_ctx *ctx);
 // full items at d = 16 but not at d = 8; NDB_TC_MIN_DIM overrides), the eps grid (row tables of <= 32 rows), eps^2 a
 // normal float far from under- and overflow, and coordinates within +-2^60 so that
 // no centred difference or squared norm overflows.  Results never depend on it.
-inline bool tc_eligible(int d, float e2, const double *lo, const double *hi, bool linked, int n_rows,
-                        uint32_t flags) {
-    static const int auto_min_dim = [] {
+inline int default_tc_min_dim() {
+    static const int v = [] {
         const char *s = getenv("NDB_TC_MIN_DIM");
-        const int v = s ? atoi(s) : 12;
-        return v < tc::kMinDim ? tc::kMinDim : v;
+        const int x = s ? atoi(s) : 12;
+        return x < tc::kMinDim ? tc::kMinDim : x;
     }();
-    // full counts scan every candidate of every point, so the tiles stay full: there
-    // the filter measured 1.17x the exact kernel already at d = 8
-    const int min_dim = (flags & (NDB_FLAG_TENSOR_FILTER | NDB_FLAG_FULL_COUNT)) ? tc::kMinDim : auto_min_dim;
+    return v;
+}
+
+inline bool tc_eligible(const ndb_ctx *ctx, int d, float e2, const double *lo, const double *hi, bool linked,
+                        int n_rows, uint32_t flags) {
+    // a context's own tuning (ndb_b200_set_tuning) applies to both count modes; by
+    // default full counts start at d = 8: they scan every candidate of every point,
+    // so the tiles stay full, and there the filter measured 1.17x the exact kernel
+    const int tuned = ctx->tuning.tc_min_dim;
+    const int min_dim = (flags & NDB_FLAG_TENSOR_FILTER) ? tc::kMinDim
+                        : tuned > 0                        ? std::max(tuned, tc::kMinDim)
+                        : (flags & NDB_FLAG_FULL_COUNT)    ? tc::kMinDim
+                                                           : default_tc_min_dim();
     if (d < min_dim || (flags & NDB_FLAG_EXACT_COUNT) || linked || n_rows > kWarp) return false;
     if (!(e2 >= 0x1p-100f && e2 <= 0x1p100f)) return false;
     for (int a = 0; a < d; ++a)
@@ -430,13 +441,18 @@ inline bool tc_eligible(int d, float e2, const double *lo, const double *hi, boo
 // kernel is faster even at d = 16.  Items with at least this many points go to the
 // tensor-core count, the rest to the exact kernel (NDB_TC_MIN_ITEM overrides it;
 // NDB_FLAG_TENSOR_FILTER sends every item).
-inline int tc_min_item() {
+inline int default_tc_min_item() {
     static const int v = [] {
         const char *s = getenv("NDB_TC_MIN_ITEM");
         const int x = s ? atoi(s) : 16;
         return x < 1 ? 1 : x;
     }();
     return v;
+}
+
+inline int ctx_tc_min_item(const ndb_ctx *ctx) {
+    const int v = ctx->tuning.tc_min_item;
+    return v <= 0 ? default_tc_min_item() : v;
 }
 
 template <int D>
@@ -480,7 +496,7 @@ void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_ite
         int2 *rest = tc_items + n_items + 1;
         ck(ctx, cudaMemsetAsync(scal + 4, 0, 2 * sizeof(uint32_t), st));
         ++launch_counter(), split_items_kernel<<<blocks_for(n_items), kBlock, 0, st>>>(
-            items, n_items, cell_start, force_tc ? 1 : tc_min_item(), tc_items, scal + 4, rest, scal + 5);
+            items, n_items, cell_start, force_tc ? 1 : ctx_tc_min_item(ctx), tc_items, scal + 4, rest, scal + 5);
         ck(ctx, cudaGetLastError());
         launch_count_tc<D>(ctx, n_items, tc_items, cell_start, nbr, n_rows, xs, e2, min_pts, early, nn_sorted, list,
                            list_cap, list_stride, jobs, cell_job, scal + 4);
@@ -770,7 +786,7 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->n_rows = pl.st.n_rows;
     ctx->cell_units = pl.cell_units ? 1 : 0;
     if (pl.st.n_rows > kWarp) return NDB_ERR_INVALID_ARGUMENT;  // row tables hold one row per lane
-    ctx->tc_count = tc_eligible(D, ctx->e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
+    ctx->tc_count = tc_eligible(ctx, D, ctx->e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
 
     classify_dispatch<D>(ctx, pl);
 
@@ -985,6 +1001,23 @@ ndb_status ndb_b200_set_memory_limit(ndb_ctx *ctx, int64_t max_bytes) {
         ctx->have_state = false;
         ctx->have_labels = false;
     }
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_set_tuning(ndb_ctx *ctx, const ndb_tuning *tuning) {
+    if (!ctx) return NDB_ERR_INVALID_ARGUMENT;
+    if (!tuning) {
+        ctx->tuning = ndb_tuning{0, 0};
+        return NDB_OK;
+    }
+    if (tuning->tc_min_dim < 0 || tuning->tc_min_item < 0) return NDB_ERR_INVALID_ARGUMENT;
+    ctx->tuning = *tuning;
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_get_tuning(ndb_ctx *ctx, ndb_tuning *tuning) {
+    if (!ctx || !tuning) return NDB_ERR_INVALID_ARGUMENT;
+    *tuning = ctx->tuning;
     return NDB_OK;
 }
 
@@ -1495,7 +1528,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
             hi[a] = jnv > 0 ? dec(h_lo_hi[(size_t)m * 2 * D + D + a]) : 0.0;
         }
         const Plan pl = plan_grid(D, jd.e2, lo, hi);
-        const bool job_tc = tc_eligible(D, jd.e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
+        const bool job_tc = tc_eligible(ctx, D, jd.e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
         double cells = 1;
         for (int a = 0; a < pl.g.k; ++a) cells *= (double)pl.g.g[a];
         bool keep = (pl.cell_units ? 1 : 0) == bp.linked && jd.min_pts - 1 <= kMaxListCap &&

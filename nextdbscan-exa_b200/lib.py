@@ -48,6 +48,8 @@ EXPORTED = (
     "ndb_b200_get_stats",
     "ndb_b200_set_memory_limit",
     "ndb_b200_device_bytes",
+    "ndb_b200_set_tuning",
+    "ndb_b200_get_tuning",
     "ndb_b200_strerror",
     "ndb_b200_last_cuda_error",
     "ndb_b200_version",
@@ -67,6 +69,12 @@ class NdbJob(ctypes.Structure):
     _fields_ = [("coords", ctypes.c_void_p), ("n", ctypes.c_int64), ("d", ctypes.c_int32),
                 ("eps", ctypes.c_float), ("min_pts", ctypes.c_int32), ("nn_out", ctypes.c_void_p),
                 ("cluster_index_out", ctypes.c_void_p), ("result", NdbResult), ("status", ctypes.c_int32)]
+
+
+class NdbTuning(ctypes.Structure):
+    """ndb_tuning: count-kernel thresholds of a context (0 = library default)."""
+
+    _fields_ = [("tc_min_dim", ctypes.c_int32), ("tc_min_item", ctypes.c_int32)]
 
 
 class NdbStats(ctypes.Structure):
@@ -148,6 +156,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbStats)]
         lib.ndb_b200_set_memory_limit.argtypes = [ctypes.c_void_p, ctypes.c_int64]
         lib.ndb_b200_device_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+        lib.ndb_b200_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbTuning)]
+        lib.ndb_b200_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbTuning)]
         lib.ndb_b200_strerror.argtypes = [ctypes.c_int]
         lib.ndb_b200_strerror.restype = ctypes.c_char_p
         lib.ndb_b200_last_cuda_error.argtypes = [ctypes.c_void_p]
@@ -155,7 +165,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_version.restype = ctypes.c_char_p
         for name in ("ndb_b200_create", "ndb_b200_destroy", "ndb_b200_set_stream", "ndb_b200_classify",
                      "ndb_b200_assign_labels", "ndb_b200_run", "ndb_b200_run_batched", "ndb_b200_cluster_label",
-                     "ndb_b200_get_stats", "ndb_b200_set_memory_limit", "ndb_b200_device_bytes"):
+                     "ndb_b200_get_stats", "ndb_b200_set_memory_limit", "ndb_b200_device_bytes",
+                     "ndb_b200_set_tuning", "ndb_b200_get_tuning"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib

@@ -65,6 +65,8 @@ def test_status_codes_without_gpu():
     assert lib.ndb_b200_create(None, 0) == 1  # null out-pointer
     assert lib.ndb_b200_set_memory_limit(None, 0) == 1
     assert lib.ndb_b200_device_bytes(None, None) == 1
+    assert lib.ndb_b200_set_tuning(None, None) == 1
+    assert lib.ndb_b200_get_tuning(None, None) == 1
     if cuda_available():
         pytest.skip("a GPU is present; the no-device path is not reachable")
     assert lib.ndb_b200_create(ctypes.byref(h), 0) == 7  # NDB_ERR_NO_DEVICE
@@ -79,3 +81,11 @@ def test_python_mirror_fails_loudly_without_device():
         pytest.skip("a GPU is present")
     with pytest.raises(pkg.lib.NdbError):
         pkg.Context(0)
+
+
+def test_autotune_candidates():
+    at = load_pkg().autotune
+    assert at.candidates(3) == []
+    c8 = at.candidates(8)
+    assert c8[0] == at.EXACT_ONLY and len(c8) == 1 + len(at.ITEM_SIZES)
+    assert all(c["tc_min_dim"] == 8 for c in c8[1:])

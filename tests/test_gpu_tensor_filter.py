@@ -118,3 +118,36 @@ def test_fill_heuristic_picks_a_kernel_and_results_agree(ctx, pkg):
     for nn, ci, res in outs[1:]:
         np.testing.assert_array_equal(nn, outs[0][0])
         np.testing.assert_array_equal(ci, outs[0][1])
+
+
+def test_tuning_and_autotuner(ctx, pkg):
+    """Per-context thresholds (ndb_b200_set_tuning) move work between the two count
+    kernels without changing a result; the autotuner times every candidate, checks
+    they agree, and leaves the fastest on the context."""
+    w = pkg.synthetic.config3(n=30_000)
+    nn_o, ci_o, _ = oracle.grid(w.coords, w.eps, w.min_pts)
+    try:
+        r = pkg.autotune.tune_count(ctx, w.coords, w.eps, w.min_pts, full_count=True, reps=2)
+        assert r["best"] in pkg.autotune.candidates(8)
+        assert ctx.tuning() == r["best"]
+        by = {(t["tc_min_dim"], t["tc_min_item"]): t for t in r["table"]}
+        assert by[(17, 0)]["tensor_items"] == 0
+        assert by[(8, 1)]["tensor_items"] > 0
+        nn, ci, _ = ctx.run(w.coords, w.eps, w.min_pts, full_count=True)
+        np.testing.assert_array_equal(nn, nn_o)
+        np.testing.assert_array_equal(ci, ci_o)
+        # early exit at d = 8: the default threshold (d >= 12) keeps the exact kernel,
+        # a tuned tc_min_dim = 8 turns the filter on
+        ctx.set_tuning(tc_min_dim=8, tc_min_item=1)
+        _, ci, _ = ctx.run(w.coords, w.eps, w.min_pts)
+        assert ctx.stats()["tensor_filter"] == 1
+        np.testing.assert_array_equal(ci, ci_o)
+        ctx.set_tuning(tc_min_dim=17)
+        nn, ci, _ = ctx.run(w.coords, w.eps, w.min_pts, full_count=True)
+        assert ctx.stats()["tensor_filter"] == 0
+        np.testing.assert_array_equal(nn, nn_o)
+        with pytest.raises(pkg.lib.NdbError, match="INVALID_ARGUMENT"):
+            ctx.set_tuning(tc_min_dim=-1)
+    finally:
+        ctx.reset_tuning()
+    assert ctx.tuning() == {"tc_min_dim": 0, "tc_min_item": 0}
