@@ -959,13 +959,13 @@ ndb_status ndb_b200_create(ndb_ctx **out, int32_t device) {
     }
     for (auto &e : ctx->ev) {
         if (cudaEventCreate(&e) != cudaSuccess) {
-            delete ctx;
+            ndb_b200_destroy(ctx);  // frees the stream and the events made so far
             return NDB_ERR_CUDA;
         }
     }
     for (auto &e : ctx->kev) {
         if (cudaEventCreate(&e) != cudaSuccess) {
-            delete ctx;
+            ndb_b200_destroy(ctx);
             return NDB_ERR_CUDA;
         }
     }
