@@ -120,6 +120,24 @@ __device__ __forceinline__ int uf_find(int *parent, int x, int *err) {
     return x;
 }
 
+// Find without path halving: no stores.  A flatten pass must use it.  There each
+// thread stores its unit's root, and a halving store by another thread (which read
+// the unit's old parent before that store) could land after it and leave an
+// intermediate ancestor behind, where the kernels that follow expect the root.
+__device__ __forceinline__ int uf_find_ro(const int *parent, int x, int *err) {
+    int p = __ldcg(parent + x);
+    int steps = 0;
+    while (p != x) {
+        x = p;
+        p = __ldcg(parent + x);
+        if (++steps > kUfMaxSteps) {
+            atomicExch(err, 1);
+            break;
+        }
+    }
+    return x;
+}
+
 __device__ __forceinline__ void uf_union(int *parent, int a, int b, int *err) {
     for (int it = 0; it < kUfMaxSteps; ++it) {
         a = uf_find(parent, a, err);

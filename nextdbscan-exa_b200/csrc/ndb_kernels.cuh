@@ -1210,10 +1210,12 @@ __global__ void union_lists_kernel(int64_t nv, const int32_t *__restrict__ nn_so
     }
 }
 
+// parent[u] = root of u.  Thread u is the only writer of parent[u] here (read-only
+// finds), so after the kernel every parent is its root.
 __global__ void flatten_kernel(int32_t *parent, int64_t n_units, int *err) {
     const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n_units) return;
-    const int r = uf_find(parent, (int)u, err);
+    const int r = uf_find_ro(parent, (int)u, err);
     parent[u] = r;
 }
 

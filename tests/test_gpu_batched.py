@@ -44,6 +44,24 @@ def test_golden_fixtures_as_one_batch(ctx, full):
             assert (nn[~below] >= m).all(), name
 
 
+def test_repeated_runs_give_the_same_ids(ctx):
+    """The union-find runs lock-free across SMs, so its timing differs from run to
+    run; the ids must not.  The golden batch and each 3-D fixture alone, many times:
+    a flatten pass whose root stores another thread could overwrite gave one point
+    of this batch a wrong id in about one run of a dozen."""
+    probs = golden_problems()
+    batch = [(g["coords"], float(g["eps"]), int(g["min_pts"])) for _, g in probs]
+    for _ in range(12):
+        for (name, g), (_, ci, _) in zip(probs, ctx.run_batched(batch)):
+            np.testing.assert_array_equal(ci, g["cluster_index"], err_msg=name)
+    for name, g in probs:
+        if g["coords"].shape[1] != 3:
+            continue
+        for _ in range(6):
+            _, ci, _ = ctx.run(g["coords"], float(g["eps"]), int(g["min_pts"]))
+            np.testing.assert_array_equal(ci, g["cluster_index"], err_msg=name)
+
+
 def test_batch_equals_single_runs(ctx, pkg):
     jobs = pkg.synthetic.config4(n_jobs=48, seed=11, n_min=200, n_max=6000)
     outs = ctx.run_batched([(j.coords, j.eps, j.min_pts) for j in jobs], full_count=True)
