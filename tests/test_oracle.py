@@ -95,3 +95,28 @@ def test_reference_harness_reproduces_fixture():
     nn, ci, lab, info = oracle.run_ref(g["coords"], float(g["eps"]), int(g["min_pts"]), threads=2)
     np.testing.assert_array_equal(nn, g["nn"])
     np.testing.assert_array_equal(ci, g["cluster_index"])
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference harness not built here")
+def test_grid_restatement_matches_reference_harness_random():
+    """Beyond the fixtures: the grid restatement against the reference's own build on
+    seeded random shapes: every d class, clustered and lattice data (many pairs exactly
+    at eps), minPts from 1 to past n."""
+    rng = np.random.default_rng(2024)
+    cases = []
+    for d in (1, 2, 3, 4, 5, 8, 12, 16):
+        n = int(rng.integers(400, 2000))
+        k = int(rng.integers(2, 12))
+        c = rng.uniform(0, 10, (k, d))
+        x = c[rng.integers(0, k, n)] + rng.normal(0, rng.uniform(0.1, 0.6), (n, d))
+        eps = float(rng.uniform(0.2, 0.9) * np.sqrt(d))
+        cases.append((x.astype(np.float32), eps, int(rng.integers(1, 3 * d + 3))))
+    for d in (2, 3):
+        g = np.stack(np.meshgrid(*[np.arange(12)] * d, indexing="ij"), -1).reshape(-1, d)
+        cases.append(((g * np.float32(0.25)).astype(np.float32), 0.25, int(2 * d)))
+    cases.append((rng.normal(0, 1, (300, 3)).astype(np.float32), 0.3, 400))
+    for x, eps, m in cases:
+        nn_r, ci_r, _, _ = oracle.run_ref(x, eps, m, threads=2)
+        nn, ci, _ = oracle.grid(x, eps, m)
+        np.testing.assert_array_equal(nn, nn_r, err_msg=f"d={x.shape[1]} eps={eps} m={m}")
+        np.testing.assert_array_equal(ci, ci_r, err_msg=f"d={x.shape[1]} eps={eps} m={m}")
