@@ -183,8 +183,12 @@ def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1,
                 times.append(time.perf_counter() - t0)
         cores = oracle.threads()
     per_step = sum(times) / len(times)
+    import inspect
+    full_n = inspect.signature(getattr(pkg.synthetic, f"config{config}")).parameters["n"].default
     return {
         "value": w.n / per_step, "unit": UNIT, "cores": cores, "kind": kind,
+        # O(n^2) work: time grows with n^2, so the rate falls with n
+        "extrapolated_value_at_full_n": w.n / per_step * w.n / full_n, "full_n": full_n,
         "sample": (f"{w.name} generator at n={w.n} (same eps={w.eps}, minPts={w.min_pts}); "
                    f"{'reference OpenMP data_process (oracle/_ref)' if kind == 'reference' else 'oracle grid port'}"
                    f", {cores} threads, {per_step:.2f} s per job; the reference is O(n^2), so its rate at the "
@@ -255,7 +259,8 @@ def run_reference_arm(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator, benchmark distribution)",
         "config": {"workload": cb["workload"], "sample": cb["sample"], "parallelism": "host OpenMP"},
-        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                            "extrapolated_value_at_full_n", "full_n") if k in cb},
         "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -401,7 +406,8 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(pkg, args.config, args.cpu_sample, os.cpu_count() or 1)
-        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                  "extrapolated_value_at_full_n", "full_n") if k in cb}
 
     launches = count_launches(s0)
     if rank == 0:
@@ -591,7 +597,8 @@ def run_ours_batch(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference_batch(pkg, os.cpu_count() or 1)
-        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                  "extrapolated_value_at_full_n", "full_n") if k in cb}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -77,3 +77,11 @@ def test_reference_arm_line_on_rank_zero(monkeypatch, capsys):
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_cpu_baseline_extrapolates_quadratically():
+    import importlib
+    pkg = importlib.import_module("nextdbscan-exa_b200")
+    cb = bench.cpu_reference(pkg, 3, 2000, 2)
+    assert cb["full_n"] == 2_000_000
+    assert cb["extrapolated_value_at_full_n"] == pytest.approx(cb["value"] * 2000 / 2_000_000)
