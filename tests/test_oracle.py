@@ -120,3 +120,30 @@ def test_grid_restatement_matches_reference_harness_random():
         nn, ci, _ = oracle.grid(x, eps, m)
         np.testing.assert_array_equal(nn, nn_r, err_msg=f"d={x.shape[1]} eps={eps} m={m}")
         np.testing.assert_array_equal(ci, ci_r, err_msg=f"d={x.shape[1]} eps={eps} m={m}")
+
+
+def test_grid_matches_literal_property():
+    """Property test of the checker itself: on arbitrary small inputs (duplicates,
+    lattice points exactly eps apart, NaN, inf, FLT_MAX, subnormals, eps of 0 or
+    negative, minPts 0 to past n) the grid restatement, which checks the GPU at large
+    n, gives the literal restatement's outputs."""
+    hyp = pytest.importorskip("hypothesis")
+    st = pytest.importorskip("hypothesis.strategies")
+    fmax = float(np.finfo(np.float32).max)
+    values = st.sampled_from([0.0, 0.25, 0.5, 0.75, 1.0, -0.5, 3.0, 1e-40, float("nan"), float("inf"),
+                              -float("inf"), fmax, 0.1, 0.2, 0.3])
+
+    @hyp.settings(max_examples=300, deadline=None, derandomize=True)
+    @hyp.given(d=st.integers(1, 16), n=st.integers(1, 40), data=st.data(),
+               eps=st.sampled_from([0.0, 0.25, 0.5, -0.5, 0.3, 1.0, 2.5]), m=st.integers(0, 8))
+    def check(d, n, data, eps, m):
+        flat = data.draw(st.lists(values, min_size=n * d, max_size=n * d))
+        x = np.array(flat, dtype=np.float32).reshape(n, d)
+        a_nn, a_ci, _, a_meta = oracle.reference(x, eps, m)
+        b_nn, b_ci, b_meta = oracle.grid(x, eps, m)
+        np.testing.assert_array_equal(a_nn, b_nn)
+        np.testing.assert_array_equal(a_ci, b_ci)
+        assert [a_meta[k] for k in ("clusters", "noise", "cores", "n")] == \
+            [b_meta[k] for k in ("clusters", "noise", "cores", "n")]
+
+    check()
