@@ -147,3 +147,28 @@ def test_grid_matches_literal_property():
             [b_meta[k] for k in ("clusters", "noise", "cores", "n")]
 
     check()
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference harness not built here")
+def test_literal_matches_reference_harness_property():
+    """The same adversarial inputs through the reference's own build: the literal
+    restatement reproduces its counts, ids and meta (single-threaded reference runs,
+    so its label sweep order is fixed)."""
+    hyp = pytest.importorskip("hypothesis")
+    st = pytest.importorskip("hypothesis.strategies")
+    fmax = float(np.finfo(np.float32).max)
+    values = st.sampled_from([0.0, 0.25, 0.5, 0.75, 1.0, -0.5, 3.0, 1e-40, float("nan"), float("inf"),
+                              -float("inf"), fmax, 0.1, 0.2, 0.3])
+
+    @hyp.settings(max_examples=60, deadline=None, derandomize=True)
+    @hyp.given(d=st.integers(1, 16), n=st.integers(1, 40), data=st.data(),
+               eps=st.sampled_from([0.0, 0.25, 0.5, -0.5, 0.3, 1.0, 2.5]), m=st.integers(0, 8))
+    def check(d, n, data, eps, m):
+        flat = data.draw(st.lists(values, min_size=n * d, max_size=n * d))
+        x = np.array(flat, dtype=np.float32).reshape(n, d)
+        r_nn, r_ci, _, _ = oracle.run_ref(x, eps, m, threads=1)
+        a_nn, a_ci, _, _ = oracle.reference(x, eps, m)
+        np.testing.assert_array_equal(a_nn, r_nn)
+        np.testing.assert_array_equal(a_ci, r_ci)
+
+    check()
