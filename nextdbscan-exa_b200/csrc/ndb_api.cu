@@ -521,7 +521,6 @@ void count_phase(ndb_ctx *ctx) {
     unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
     ensure(ctx, ctx->nn_sorted, (ctx->n + 1) * sizeof(int32_t));
     const bool early = (ctx->flags_run & NDB_FLAG_FULL_COUNT) == 0;
-    const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
     // neighbour lists for the border step: min_pts - 1 entries per point
     ctx->list_cap = 0;
     const int64_t cap = (int64_t)ctx->min_pts - 1;
@@ -1278,7 +1277,6 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         ensure(ctx, ctx->nbr_list, (size_t)(nv * bp.list_stride + 1) * sizeof(int32_t));
         list = ctx->nbr_list.as<int32_t>();
     }
-    const unsigned grid = (unsigned)((n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
     const bool early = (flags & NDB_FLAG_FULL_COUNT) == 0;
     cudaEventRecord(ctx->ev[1], st);
     cudaEventRecord(ctx->kev[2], st);
