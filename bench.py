@@ -161,7 +161,7 @@ def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1,
 
     if not oracle.have_ref():
         try:
-            oracle.build("/root/reference" if os.path.isdir("/root/reference") else None)
+            oracle.build()
         except Exception:
             pass
     w = pkg.synthetic.make(config, n=sample_n)
@@ -210,7 +210,7 @@ def cpu_reference_batch(pkg, threads: int, steps: int = 1, warmup: int = 0):
 
     if not oracle.have_ref():
         try:
-            oracle.build("/root/reference" if os.path.isdir("/root/reference") else None)
+            oracle.build()
         except Exception:
             pass
     jobs = batch_sample(pkg)

@@ -213,6 +213,15 @@ ndb_status ndb_b200_set_tuning(ndb_ctx *ctx, const ndb_tuning *tuning);
 /* The context's thresholds as set (0 where the default applies). */
 ndb_status ndb_b200_get_tuning(ndb_ctx *ctx, ndb_tuning *tuning);
 
+/* Bound of the device-side union-find loops of the context's runs: steps of one
+ * find and attempts of one union (0 = the default, 2^26).  A loop that reaches it
+ * ends, and the run returns NDB_ERR_DEVICE_LIMIT instead of spinning; its outputs
+ * are then undefined, and the context stays usable.  The default is far above any
+ * depth lock-free hooking reaches; small values exist so that tests can make the
+ * bound run out on purpose.  No counterpart in the reference, whose propagation
+ * loop (data_process.cpp:183) has no bound. */
+ndb_status ndb_b200_set_debug_limits(ndb_ctx *ctx, int64_t uf_max_steps);
+
 /* Device bytes the context holds now (its buffers grow to the largest job run and
  * are kept until ndb_b200_destroy or a lower memory cap). */
 ndb_status ndb_b200_device_bytes(ndb_ctx *ctx, int64_t *bytes);

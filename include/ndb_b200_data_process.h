@@ -4,7 +4,7 @@
 //
 // Same constructor arguments, same phase methods, same public result vectors,
 // so nextdbscan::start (nextdbscan.cpp:46-58) and main.cpp compile unchanged when
-// the reference's data_process.h selects this header.  The
+// the reference's data_process.h includes this header in place of its own class.  The
 // methods are noexcept like the reference's; a failing status is printed to
 // std::cerr and ends the process with EXIT_FAILURE, which is how the reference
 // treats hard errors (magma_input.h:158-159, data_process.cpp:38-41).

@@ -216,6 +216,15 @@ class Context:
         lib.check(self._lib.ndb_b200_get_tuning(self._h, ctypes.byref(t)), "ndb_b200_get_tuning", self._h)
         return {"tc_min_dim": t.tc_min_dim, "tc_min_item": t.tc_min_item}
 
+    def set_debug_limits(self, uf_max_steps: int = 0) -> None:
+        """Bound of the device-side union-find loops (0 = the library default); a run
+        that reaches it raises NdbError(NDB_ERR_DEVICE_LIMIT) and leaves the context
+        usable.  For tests of that error path."""
+        if uf_max_steps < 0:
+            raise ValueError("uf_max_steps must be >= 0")
+        lib.check(self._lib.ndb_b200_set_debug_limits(self._h, int(uf_max_steps)), "ndb_b200_set_debug_limits",
+                  self._h)
+
     def device_bytes(self) -> int:
         """Device memory the context holds now."""
         out = ctypes.c_int64()

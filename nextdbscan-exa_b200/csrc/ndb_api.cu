@@ -55,6 +55,8 @@ struct ndb_ctx {
     size_t mem_limit = 0;
     // count-kernel thresholds set by ndb_b200_set_tuning (0: the library's defaults)
     ndb_tuning tuning{0, 0};
+    // bound of the device-side union-find loops (ndb_b200_set_debug_limits; 0: kUfMaxSteps)
+    int uf_max_steps = 0;
 
     template <typename F>
     void for_each_buf(F f) {
@@ -758,7 +760,8 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     // bounding box of the grid-eligible points
     int *lo_hi = small_at<int>(ctx, kSmallBboxOff);
     unsigned long long *n_invalid = small_at<unsigned long long>(ctx, kSmallInvalidOff);
-    ++launch_counter(), bbox_init_kernel<<<1, 32, 0, st>>>(lo_hi, D, n_invalid);
+    ++launch_counter(), bbox_init_kernel<<<1, 32, 0, st>>>(lo_hi, D, n_invalid, small_at<int>(ctx, kSmallErrOff),
+                                                           ctx->uf_max_steps);
     ++launch_counter(), bbox_kernel<D><<<std::min<unsigned>(blocks_for(n), 148 * 8), kBlock, 0, st>>>(ctx->coords_dev, n, lo_hi,
                                                                                   n_invalid);
     ck(ctx, cudaGetLastError());
@@ -1011,6 +1014,12 @@ ndb_status ndb_b200_set_tuning(ndb_ctx *ctx, const ndb_tuning *tuning) {
     }
     if (tuning->tc_min_dim < 0 || tuning->tc_min_item < 0) return NDB_ERR_INVALID_ARGUMENT;
     ctx->tuning = *tuning;
+    return NDB_OK;
+}
+
+ndb_status ndb_b200_set_debug_limits(ndb_ctx *ctx, int64_t uf_max_steps) {
+    if (!ctx || uf_max_steps < 0 || uf_max_steps > INT32_MAX) return NDB_ERR_INVALID_ARGUMENT;
+    ctx->uf_max_steps = (int)uf_max_steps;
     return NDB_OK;
 }
 
@@ -1630,6 +1639,9 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     launch_counter() = 0;
     if (grow(ctx, ctx->small, kSmallBytes) != cudaSuccess) return NDB_ERR_OUT_OF_MEMORY;
     if (cudaMemsetAsync(ctx->small.ptr, 0, kSmallBytes, ctx->stream) != cudaSuccess) return NDB_ERR_CUDA;
+    ++launch_counter(), set_int_kernel<<<1, 1, 0, ctx->stream>>>(small_at<int>(ctx, kSmallErrOff) + 1,
+                                                                 ctx->uf_max_steps);
+    if (cudaGetLastError() != cudaSuccess) return NDB_ERR_CUDA;
     ndb_status first = NDB_OK;
     // validate, and group by dimensionality
     std::vector<std::vector<int>> groups(NDB_MAX_DIM + 1);
@@ -1749,7 +1761,6 @@ namespace {
 
 constexpr size_t na_align(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kNaN = NDB_NOALLOC_MAX_POINTS;
-constexpr int kNaMaxRows = 27;  // largest stencil plan_grid builds (4 gridded dimensions: 3^3 rows)
 
 // Capacity of each buffer for jobs of up to kNaN points (upper bounds of the
 // requests the pipeline makes: keys may be 64-bit, coordinates padded to 16).
@@ -1766,7 +1777,7 @@ constexpr size_t na_cap(int b) {
          : b == NA_XS ? 4 * 16 * (kNaN + 1)
          : b == NA_CELL_START ? 4 * (kNaN + 2)
          : b == NA_CELL_KEY || b == NA_ITEMS ? 8 * (kNaN + 1)
-         : b == NA_NBR ? 8 * (kMaxRows > kNaMaxRows ? kNaMaxRows : kMaxRows) * kNaN + 8
+         : b == NA_NBR ? 8 * kWarp * kNaN + 8  // classify refuses stencils of more than kWarp rows
          : b == NA_CORE_SORTED || b == NA_CELL_HAS_CORE ? kNaN + 1
          : b == NA_SORT_HIST ? 4 * 256 * ((kNaN + kSortTile - 1) / kSortTile)
          : b == NA_SCAN ? 4 * 4096
@@ -1848,10 +1859,21 @@ extern "C" ndb_status ndb_b200_run_noalloc(const float *coords, int64_t n, int32
             cudaGetLastError();
             return NDB_ERR_CUDA;
         }
-        for (auto &ev : s.ctx.ev)
-            if (cudaEventCreate(&ev) != cudaSuccess) return NDB_ERR_CUDA;
-        for (auto &ev : s.ctx.kev)
-            if (cudaEventCreate(&ev) != cudaSuccess) return NDB_ERR_CUDA;
+        // the timing events, kept only once all of them exist (a failed attempt
+        // leaves nothing behind, so a retry starts clean)
+        constexpr int kNev = sizeof(s.ctx.ev) / sizeof(s.ctx.ev[0]), kNkev = sizeof(s.ctx.kev) / sizeof(s.ctx.kev[0]);
+        cudaEvent_t evs[kNev + kNkev] = {};
+        for (int i = 0; i < kNev + kNkev; ++i) {
+            e = cudaEventCreate(&evs[i]);
+            if (e != cudaSuccess) {
+                s.ctx.last_cuda_error = cudaGetErrorString(e);
+                for (int k = 0; k < i; ++k) cudaEventDestroy(evs[k]);
+                cudaGetLastError();
+                return NDB_ERR_CUDA;
+            }
+        }
+        for (int i = 0; i < kNev; ++i) s.ctx.ev[i] = evs[i];
+        for (int i = 0; i < kNkev; ++i) s.ctx.kev[i] = evs[kNev + i];
         s.base = static_cast<unsigned char *>(addr);
         s.ctx.device = dev;
         s.ready = true;
@@ -1866,5 +1888,12 @@ extern "C" ndb_status ndb_b200_run_noalloc(const float *coords, int64_t n, int32
     ndb_status st = ndb_b200_classify(&s.ctx, coords, n, d, eps, min_pts, flags | NDB_FLAG_DEVICE_PTRS, nn_out);
     if (st == NDB_OK) st = ndb_b200_assign_labels(&s.ctx, cluster_index_out, result);
     if (!na_inside(s, s.ctx)) st = NDB_ERR_OUT_OF_MEMORY;  // a request outgrew its slice
+    if (st != NDB_OK) {
+        // a failure can return with kernels still queued on the array: wait for
+        // them, so that every call is complete on return and the next one (from
+        // any stream) finds the array idle
+        cudaStreamSynchronize(s.ctx.stream);
+        cudaGetLastError();
+    }
     return st;
 }

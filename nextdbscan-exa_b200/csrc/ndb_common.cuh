@@ -101,18 +101,31 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // Lock-free union-find over int32 ids.  parent[x] <= x always (the larger root
 // is hooked under the smaller), so every find terminates.  Reads go through L2
 // (ld.cg) because other SMs rewrite parents concurrently.
+//
+// Every loop is bounded.  err[0] is the run's error flag; err[1] holds the bound
+// (steps of one find, attempts of one union), written by the host before the run
+// (0 means the default kUfMaxSteps).  A loop that reaches it sets err[0] and
+// returns, so the host reports NDB_ERR_DEVICE_LIMIT instead of a hung kernel.  The
+// bound is never written while a kernel runs, so it is read through the
+// read-only path.
 // ---------------------------------------------------------------------------
 constexpr int kUfMaxSteps = 1 << 26;
 
+__device__ __forceinline__ int uf_limit(const int *err) {
+    const int v = __ldg(err + 1);
+    return v > 0 ? v : kUfMaxSteps;
+}
+
 __device__ __forceinline__ int uf_find(int *parent, int x, int *err) {
     int p = __ldcg(parent + x);
+    const int lim = uf_limit(err);
     int steps = 0;
     while (p != x) {
         const int gp = __ldcg(parent + p);
         if (gp != p) __stcg(parent + x, gp);  // path halving: gp is an ancestor of x
         x = p;
         p = gp;
-        if (++steps > kUfMaxSteps) {
+        if (++steps > lim) {
             atomicExch(err, 1);
             break;
         }
@@ -126,11 +139,12 @@ __device__ __forceinline__ int uf_find(int *parent, int x, int *err) {
 // intermediate ancestor behind, where the kernels that follow expect the root.
 __device__ __forceinline__ int uf_find_ro(const int *parent, int x, int *err) {
     int p = __ldcg(parent + x);
+    const int lim = uf_limit(err);
     int steps = 0;
     while (p != x) {
         x = p;
         p = __ldcg(parent + x);
-        if (++steps > kUfMaxSteps) {
+        if (++steps > lim) {
             atomicExch(err, 1);
             break;
         }
@@ -139,7 +153,8 @@ __device__ __forceinline__ int uf_find_ro(const int *parent, int x, int *err) {
 }
 
 __device__ __forceinline__ void uf_union(int *parent, int a, int b, int *err) {
-    for (int it = 0; it < kUfMaxSteps; ++it) {
+    const int lim = uf_limit(err);
+    for (int it = 0; it < lim; ++it) {
         a = uf_find(parent, a, err);
         b = uf_find(parent, b, err);
         if (a == b) return;

@@ -106,14 +106,20 @@ __device__ __forceinline__ int ordered_int(float f) {
     return i >= 0 ? i : i ^ 0x7fffffff;
 }
 
-__global__ void bbox_init_kernel(int *lo_hi, int d, unsigned long long *n_invalid) {
+// Also writes the union-find bound of the run (err[1], see uf_limit).
+__global__ void bbox_init_kernel(int *lo_hi, int d, unsigned long long *n_invalid, int *err, int uf_limit) {
     const int t = threadIdx.x;
     if (t < d) {
         lo_hi[t] = 0x7fffffff;
         lo_hi[d + t] = (int)0x80000000;
     }
-    if (t == 0) *n_invalid = 0ull;
+    if (t == 0) {
+        *n_invalid = 0ull;
+        err[1] = uf_limit;
+    }
 }
+
+__global__ void set_int_kernel(int *p, int v) { *p = v; }
 
 // lo_hi[0..D) = ordered-int min, lo_hi[D..2D) = ordered-int max.
 template <int D>

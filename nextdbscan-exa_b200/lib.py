@@ -50,6 +50,8 @@ EXPORTED = (
     "ndb_b200_device_bytes",
     "ndb_b200_set_tuning",
     "ndb_b200_get_tuning",
+    "ndb_b200_set_debug_limits",
+    "ndb_b200_run_noalloc",
     "ndb_b200_strerror",
     "ndb_b200_last_cuda_error",
     "ndb_b200_version",
@@ -158,6 +160,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_device_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
         lib.ndb_b200_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbTuning)]
         lib.ndb_b200_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbTuning)]
+        lib.ndb_b200_set_debug_limits.argtypes = [ctypes.c_void_p, ctypes.c_int64]
         lib.ndb_b200_strerror.argtypes = [ctypes.c_int]
         lib.ndb_b200_strerror.restype = ctypes.c_char_p
         lib.ndb_b200_last_cuda_error.argtypes = [ctypes.c_void_p]
@@ -166,7 +169,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         for name in ("ndb_b200_create", "ndb_b200_destroy", "ndb_b200_set_stream", "ndb_b200_classify",
                      "ndb_b200_assign_labels", "ndb_b200_run", "ndb_b200_run_batched", "ndb_b200_cluster_label",
                      "ndb_b200_get_stats", "ndb_b200_set_memory_limit", "ndb_b200_device_bytes",
-                     "ndb_b200_set_tuning", "ndb_b200_get_tuning"):
+                     "ndb_b200_set_tuning", "ndb_b200_get_tuning", "ndb_b200_set_debug_limits"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
         return lib

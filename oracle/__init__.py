@@ -27,11 +27,25 @@ NO_CLUSTER = 2**31 - 1
 _lib = None
 
 
-def build(ref_dir: str | None = None) -> None:
+def ref_dir() -> str | None:
+    """Where the reference's sources are checked out: $NDB_REF_DIR, else the
+    read-only mount this repository's build reads them from.  None when neither
+    holds data_process.cpp (for instance on a GPU box, which only runs the
+    prebuilt _ref/ binaries)."""
+    for cand in (os.environ.get("NDB_REF_DIR"), "/root/reference"):
+        if cand and os.path.isfile(os.path.join(cand, "data_process.cpp")):
+            return cand
+    return None
+
+
+def build(ref: str | None = None, targets: tuple[str, ...] = ()) -> None:
+    """Builds the C restatement and, when the reference's sources are found, the
+    reference's own OpenMP build into _ref/."""
     cmd = ["make", "-s", "-C", HERE]
-    if ref_dir:
-        cmd.append(f"REF_DIR={ref_dir}")
-    subprocess.run(cmd, check=True)
+    ref = ref or ref_dir()
+    if ref:
+        cmd.append(f"REF_DIR={ref}")
+    subprocess.run(cmd + list(targets), check=True)
 
 
 def _load() -> ctypes.CDLL:

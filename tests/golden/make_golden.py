@@ -122,10 +122,10 @@ def sha(a: np.ndarray) -> str:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-dir", default="/root/reference")
+    ap.add_argument("--ref-dir", default=None, help="reference checkout (default: $NDB_REF_DIR or the build's mount)")
     ap.add_argument("--skip-full", action="store_true")
     args = ap.parse_args()
-    oracle.build(args.ref_dir)
+    oracle.build(args.ref_dir or oracle.ref_dir())
     if not oracle.have_ref():
         raise SystemExit("reference harness could not be built")
     for name, x, eps, m in cases():

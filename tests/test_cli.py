@@ -128,3 +128,54 @@ def test_cli_labels_and_dropin_vectors_match_reference(binaries, tmp_path, name)
     raw = np.fromfile(vec, dtype=np.int32)
     np.testing.assert_array_equal(raw[:n], g["nn"])
     np.testing.assert_array_equal(raw[n:], g["cluster_index"])
+
+
+# ---------------------------------------------------------------------------
+# The reference's own caller: main.cpp and nextdbscan.cpp compiled unchanged, with
+# the -DB200_ON switch added to a copy of its data_process.h (oracle/Makefile,
+# target dropin), linked against libndb_b200.so.  The binary is built where the
+# reference's sources are; elsewhere the prebuilt one is used.
+# ---------------------------------------------------------------------------
+REF_DROPIN = os.path.join(ROOT, "oracle", "_ref", "nextdbscan-dropin")
+
+
+def _ref_dropin():
+    import oracle
+
+    if oracle.ref_dir():
+        oracle.build(targets=("dropin",))
+    if not os.path.exists(REF_DROPIN):
+        pytest.skip("the reference's caller is not built here (no reference sources, no prebuilt binary)")
+    return REF_DROPIN
+
+
+def test_reference_caller_builds_against_the_dropin(tmp_path):
+    exe = _ref_dropin()
+    r = subprocess.run([exe, "-m", "5", str(tmp_path / "x.bin")], capture_output=True, text=True)
+    assert r.returncode != 0 and "specify the m and e" in r.stdout  # main.cpp:80-84
+    if _cuda_available():
+        return
+    g = load_golden("c1_n4000")
+    p = tmp_path / "c1.bin"
+    _write_bin(p, g["coords"])
+    r = subprocess.run([exe, "-m", "5", "-e", "0.8", "-t", "1", str(p)], capture_output=True, text=True)
+    assert r.returncode != 0 and "no CUDA device" in r.stderr, r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c1_n4000", "blobs_d3", "blobs_d8", "blobs_d16", "border_tie", "all_noise"])
+def test_reference_caller_prints_the_reference_meta(tmp_path, name):
+    """The reference's main.cpp through nextdbscan::start (nextdbscan.cpp:46-58) on the
+    drop-in prints the clusters, core points and noise points of the reference's own
+    run (main.cpp:98-106)."""
+    exe = _ref_dropin()
+    g = load_golden(name)
+    p = tmp_path / f"{name}.bin"
+    _write_bin(p, g["coords"])
+    eps, m = repr(float(np.float32(g["eps"]))), str(int(g["min_pts"]))
+    r = subprocess.run([exe, "-m", m, "-e", eps, "-t", "1", str(p)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    clusters, noise, cores, n = (int(v) for v in g["meta"])
+    assert f"Read {n} aggregated points" in r.stdout
+    assert f"Estimated Clusters: {clusters}" in r.stdout
+    assert f"Core Points: {cores}" in r.stdout and f"Noise Points: {noise}" in r.stdout
