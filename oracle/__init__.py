@@ -6,6 +6,7 @@ thing measured on the GPU or shipped.
 
   reference(...)  literal restatement of the reference's phases (ndb_oracle.c)
   grid(...)       exact grid restatement of the same outputs (ndb_oracle.c)
+  cells(...)      the same outputs organised for 10^7..10^8 points (ndb_oracle.c)
   run_ref(...)    the reference's own OpenMP implementation, built from its
                   sources into _ref/ndb_ref_harness by oracle/Makefile
 """
@@ -61,6 +62,9 @@ def _load() -> ctypes.CDLL:
         lib.ndb_oracle_grid.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
                                         vp, vp, vp]
         lib.ndb_oracle_grid.restype = ctypes.c_int
+        lib.ndb_oracle_cells.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
+                                         ctypes.c_int32, vp, vp, vp]
+        lib.ndb_oracle_cells.restype = ctypes.c_int
         lib.ndb_oracle_threads.restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -101,6 +105,24 @@ def grid(coords, eps: float, min_pts: int):
     if rc != 0:
         raise RuntimeError(f"ndb_oracle_grid failed: {rc}")
     return nn, ci, dict(clusters=int(meta[0]), noise=int(meta[1]), cores=int(meta[2]), n=int(meta[3]))
+
+
+def cells(coords, eps: float, min_pts: int, early: bool = False):
+    """Cell restatement (exact, OpenMP in every phase, for 10^7..10^8 points).
+    Same outputs as grid(); with early=True a point stops counting at min_pts, so
+    nn is exact below min_pts and some value >= min_pts otherwise (core flags,
+    cluster ids and meta stay exact).  Returns (nn, cluster_index, meta dict)."""
+    a = _pts(coords)
+    n, d = a.shape
+    nn = np.zeros(n, np.int32)
+    ci = np.zeros(n, np.int32)
+    meta = np.zeros(8, np.int32)
+    rc = _load().ndb_oracle_cells(a.ctypes.data, n, d, ctypes.c_float(eps), int(min_pts), int(bool(early)),
+                                  nn.ctypes.data, ci.ctypes.data, meta.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ndb_oracle_cells failed: {rc}")
+    return nn, ci, dict(clusters=int(meta[0]), noise=int(meta[1]), cores=int(meta[2]), n=int(meta[3]),
+                        clique_cells=bool(meta[4]))
 
 
 def threads() -> int:
