@@ -1,16 +1,28 @@
 #!/usr/bin/env python
-"""Benchmark: clustered points/s of the B200 DBSCAN hot path.
+"""Benchmark: clustered points/s of the B200 DBSCAN hot path, chosen form against
+the plain GPU form.
 
-One step = one full DBSCAN job (epsilon grid, neighbour count / core flags,
-union-find, canonical ids, border points) over the n=10,000,000 3-D workload
-(seeded synthetic data with the benchmark's distribution), inputs resident in HBM.
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C]
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Default (configuration 4): one step = the 4,096-job batch (n log-uniform in
+[1k, 200k], d in {2, 3, 8, 16}, 151M points, seeded synthetic data with the
+benchmark's distribution) through ndb_b200_run_batched, inputs resident in HBM.
+The same line carries, each measured in the same run:
+  plain_gpu_form        the same jobs as one ndb_b200_run call each (the plain
+                        GPU form the batched form is chosen over);
+  tensor_filter_8d_2m   the 8-D 2M-point workload with the exact FP32 count (the
+                        plain form), the tensor-core filtered count and the
+                        library's automatic choice, in both count modes, with the
+                        filter's guard-band population and an audit of every pair
+                        it classified against FP64 distances and the exact
+                        predicate;
+  plain_3d_10m          the 10M-point 3-D workload on the plain path.
+--config 1|2|3|5 times that one workload alone.
 
-N > 1 runs under torchrun, one process per GPU: the path does not shard on one
-job here (one GPU is one rank), so every rank runs an independent replica of the
-job and the value is the points all ranks clustered / the max over ranks of the
-timed device time ("scaling": "weak").
+N > 1 runs under torchrun, one process per GPU: independent jobs do not need a
+collective, so every rank runs its own replica of the step and the value is the
+points all ranks clustered / the max over ranks of the timed device time
+("scaling": "weak").
 
 --impl reference times the reference's own OpenMP implementation (built from its
 sources into oracle/_ref/) on the host cores, on a bounded sample of the same
@@ -35,6 +47,7 @@ UNIT = "points/s"
 HBM_PEAK_FALLBACK = 6650.0  # GB/s, used only without MEASURED_PEAKS.json
 SM_COUNT = 148
 FP32_LANES_PER_SM = 128
+BATCH_JOBS = 4096
 
 
 def parse():
@@ -43,18 +56,20 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", type=int, default=2, help="benchmark configuration (1..5; 4 is the batched one)")
+    ap.add_argument("--config", type=int, default=4, help="benchmark configuration (1..5; 4, the default, is the batch)")
     ap.add_argument("--n", type=int, default=None, help="override n (smaller runs for profiling)")
     ap.add_argument("--full-count", action="store_true", help="exact neighbour counts (no early exit)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="configuration 4: skip the 8-D and 3-D workloads carried in the same line")
     ap.add_argument("--cpu-sample", type=int, default=50_000, help="points in the bounded CPU sample")
-    ap.add_argument("--jobs", type=int, default=4096, help="jobs of the batched configuration 4")
+    ap.add_argument("--jobs", type=int, default=BATCH_JOBS, help="jobs of the batched configuration 4")
     ap.add_argument("--count-kernel", choices=["auto", "exact", "tensor"], default="auto",
                     help="neighbour-count kernel for d >= 8: picked per item (auto), exact FP32 only, or tensor filter")
     ap.add_argument("--autotune", action="store_true",
                     help="d >= 8: pick the count-kernel thresholds on the workload before timing")
-    ap.add_argument("--no-plain", action="store_true", help="configuration 4: skip the one-call-per-job form")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparisons")
     ap.add_argument("--dims", type=str, default=None,
                     help="configuration 4: keep only the jobs of these dimensionalities (comma list)")
     ap.add_argument("--max-jobs", type=int, default=None, help="configuration 4: keep at most this many jobs")
@@ -97,6 +112,7 @@ class ClockSampler:
             self._stop.wait(0.2)
 
     def __enter__(self):
+        self._stop.clear()
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
         return self
@@ -156,7 +172,7 @@ def barrier(world: int):
 # ---------------------------------------------------------------------------
 # reference arm: the reference's own OpenMP implementation on the host cores
 # ---------------------------------------------------------------------------
-def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1, warmup: int = 0):
+def _ensure_ref():
     import oracle
 
     if not oracle.have_ref():
@@ -164,7 +180,14 @@ def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1,
             oracle.build()
         except Exception:
             pass
-    w = pkg.synthetic.make(config, n=sample_n)
+    return oracle
+
+
+def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1, warmup: int = 0):
+    oracle = _ensure_ref()
+    import inspect
+    full_n = inspect.signature(getattr(pkg.synthetic, f"config{config}")).parameters["n"].default
+    w = pkg.synthetic.make(config, n=min(sample_n, full_n))
     if oracle.have_ref():
         kind = "reference"
         times = []
@@ -183,16 +206,17 @@ def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1,
                 times.append(time.perf_counter() - t0)
         cores = oracle.threads()
     per_step = sum(times) / len(times)
-    import inspect
-    full_n = inspect.signature(getattr(pkg.synthetic, f"config{config}")).parameters["n"].default
+    whole = w.n == full_n
     return {
         "value": w.n / per_step, "unit": UNIT, "cores": cores, "kind": kind,
         # O(n^2) work: time grows with n^2, so the rate falls with n
         "extrapolated_value_at_full_n": w.n / per_step * w.n / full_n, "full_n": full_n,
-        "sample": (f"{w.name} generator at n={w.n} (same eps={w.eps}, minPts={w.min_pts}); "
-                   f"{'reference OpenMP data_process (oracle/_ref)' if kind == 'reference' else 'oracle grid port'}"
-                   f", {cores} threads, {per_step:.2f} s per job; the reference is O(n^2), so its rate at the "
-                   f"full n is lower by about n_full/n_sample"),
+        "sample": ((f"the whole {w.name} workload (n={w.n}, eps={w.eps}, minPts={w.min_pts})" if whole else
+                    f"{w.name} generator at n={w.n} (same eps={w.eps}, minPts={w.min_pts})") +
+                   f"; {'reference OpenMP data_process (oracle/_ref)' if kind == 'reference' else 'oracle grid port'}"
+                   f", {cores} threads, {per_step:.2f} s per job" +
+                   ("" if whole else "; the reference is O(n^2), so its rate at the full n is lower by about "
+                                     "n_full/n_sample")),
         "seconds_per_step": per_step,
         "workload": w.name,
     }
@@ -206,13 +230,7 @@ def batch_sample(pkg, n_jobs: int = 24, n_cap: int = 40_000):
 
 
 def cpu_reference_batch(pkg, threads: int, steps: int = 1, warmup: int = 0):
-    import oracle
-
-    if not oracle.have_ref():
-        try:
-            oracle.build()
-        except Exception:
-            pass
+    oracle = _ensure_ref()
     jobs = batch_sample(pkg)
     pts = sum(j.n for j in jobs)
     times = []
@@ -230,13 +248,20 @@ def cpu_reference_batch(pkg, threads: int, steps: int = 1, warmup: int = 0):
             times.append(t)
     per_step = sum(times) / len(times)
     cores = threads if kind == "reference" else oracle.threads()
+    # the reference's time per job grows with n^2: the whole batch takes
+    # per_step * sum(n^2 over the batch) / sum(n^2 over the sample)
+    shapes = pkg.synthetic.config4_shapes(n_jobs=BATCH_JOBS)
+    full_pts = sum(n for n, _ in shapes)
+    full_sq = sum(float(n) * n for n, _ in shapes)
+    sample_sq = sum(float(j.n) * j.n for j in jobs)
     return {
         "value": pts / per_step, "unit": UNIT, "cores": cores, "kind": kind,
+        "extrapolated_value_at_full_n": full_pts / (per_step * full_sq / sample_sq), "full_n": full_pts,
         "sample": (f"the first {len(jobs)} jobs with n <= 40,000 of the 4,096-job batch ({pts} points, "
                    f"d in {sorted({j.d for j in jobs})}); "
                    f"{'reference OpenMP data_process (oracle/_ref)' if kind == 'reference' else 'oracle grid port'}"
                    f", one job after another, {cores} threads, {per_step:.2f} s; the reference is O(n^2) per job, "
-                   f"so on the full batch (mean n 37k, up to 200k) its rate is lower"),
+                   f"so the whole batch (mean n 37k, up to 200k) is extrapolated by the sum of n^2"),
         "seconds_per_step": per_step,
         "workload": "batched-4096-jobs",
     }
@@ -270,10 +295,168 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def timed(fn, steps: int, flush, stream) -> list[float]:
+    """Device time (ms) of fn() per step on the library's stream, L2 flushed before
+    each step (not timed)."""
+    import torch
+    out = []
+    for _ in range(steps):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def kernel_times(stats: list[dict]) -> dict:
+    return {
+        "count_kernel": statistics.mean(s["ms_count_kernel"] for s in stats),
+        "union_kernel": statistics.mean(s["ms_union_kernel"] for s in stats),
+        "border_kernel": statistics.mean(s["ms_border_kernel"] for s in stats),
+        "radix_sort": statistics.mean(s["ms_sort_kernels"] for s in stats),
+    }
+
+
+def measure_workload(pkg, ctx, w, steps: int, warmup: int, flush, stream, full: bool, ck_kw: dict, e2e: bool,
+                     world: int, clk=None) -> dict:
+    """One workload on the single-job path: device-resident steps, then the same
+    job through the public call with pinned host buffers (e2e)."""
+    import torch
+    n, d = w.n, w.d
+    x = torch.from_numpy(w.coords).cuda()
+    nn = torch.empty(n, dtype=torch.int32, device="cuda")
+    ci = torch.empty(n, dtype=torch.int32, device="cuda")
+    box = {"stats": []}
+
+    def step():
+        box["res"] = ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(),
+                                    full_count=full, **ck_kw)
+        box["stats"].append(ctx.stats())
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    box["stats"] = []
+    if clk is not None:
+        with clk:
+            ms = timed(step, steps, flush, stream)
+    else:
+        ms = timed(step, steps, flush, stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    value, total_ms = whole_job_rate(n, steps, sum(ms), world)
+    out = {"value": value, "ms_per_step": total_ms / steps, "res": box["res"], "stats": box["stats"]}
+    if e2e:
+        hx = torch.from_numpy(w.coords).pin_memory()
+        hnn = torch.empty(n, dtype=torch.int32).pin_memory()
+        hci = torch.empty(n, dtype=torch.int32).pin_memory()
+
+        def e2e_step():
+            ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
+                         full_count=full, **ck_kw)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        e_ms = timed(e2e_step, steps, flush, stream)
+        e_total = max_over_ranks(sum(e_ms), world)
+        out["e2e"] = {"value": world * n * steps / (e_total / 1000.0), "unit": UNIT,
+                      "h2d_bytes_per_step": n * d * 4, "d2h_bytes_per_step": 2 * n * 4}
+    return out
+
+
+def roofline_of(stats: list[dict], n: int, workload: str, clk: dict) -> dict:
+    """Roofline of the dominant kernel of a measured workload."""
+    hbm_peak, peak_src = peaks()
+    kern = kernel_times(stats)
+    s0 = stats[-1]
+    dominant = max(kern, key=kern.get)
+    roof = roofline(dominant, kern[dominant], s0, n, hbm_peak, peak_src, clk)
+    tkey = "tensor_count_kernel" if (dominant == "count_kernel" and s0["tensor_items"]) else dominant
+    roof["traffic"] = traffic_per_launch(workload, tkey, n)
+    roof["traffic_source"] = "profiles/traffic_per_launch.md (ncu capture, scaled by n)" if roof["traffic"] else None
+    return roof
+
+
+def summary_of(stats: list[dict]) -> dict:
+    s0 = stats[-1]
+    return {
+        "phases_ms": {k: round(statistics.mean(s[k] for s in stats), 4)
+                      for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
+        "kernels_ms": {k: round(v, 4) for k, v in kernel_times(stats).items()},
+        "pairs": {"count": s0["count_pairs"], "union": s0["union_pairs"], "border": s0["border_pairs"]},
+        "grid": {"cells": s0["n_cells"], "tiles": s0["n_tiles"], "rows": s0["stencil_rows"],
+                 "same_cell_linked": s0["same_cell_linked"], "key_bits": s0["key_bits"]},
+        "kernel_launches_per_step": s0["kernel_launches"],
+    }
+
+
+def tensor_filter_forms(pkg, ctx, steps: int, flush, stream) -> dict:
+    """The 8-D 2M-point workload: the exact FP32 count (the plain form), the
+    tensor-core filtered count and the library's automatic choice, in both count
+    modes, each timed on device-resident inputs with identical ids checked; then one
+    audited run of the filter (NDB_FLAG_FILTER_AUDIT, untimed)."""
+    import numpy as np
+    import torch
+    w = pkg.synthetic.config3()
+    n, d = w.n, w.d
+    x = torch.from_numpy(w.coords).cuda()
+    nn = torch.empty(n, dtype=torch.int32, device="cuda")
+    ci = torch.empty(n, dtype=torch.int32, device="cuda")
+    out = {"workload": w.name, "n": n, "d": d, "eps": w.eps, "min_pts": w.min_pts,
+           "l2": "flushed between timed steps", "steps": steps}
+    for mode, full in (("early_exit", False), ("full_counts", True)):
+        forms, ref = {}, None
+        for name, kw in (("exact_fp32_count", {"exact_count": True}), ("tensor_filter_count", {"tensor_filter": True}),
+                         ("chosen", {})):
+            def run(kw=kw):
+                ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(), full_count=full,
+                               **kw)
+            run()
+            torch.cuda.synchronize()
+            ms = timed(run, steps, flush, stream)
+            s = ctx.stats()
+            ids = ci.cpu().numpy()
+            if ref is None:
+                ref = (ids, nn.cpu().numpy())
+            f = {"value": n * len(ms) / (sum(ms) / 1000.0), "unit": UNIT, "ms_per_step": sum(ms) / len(ms),
+                 "count_kernel_ms": s["ms_count_kernel"], "tensor_filter": bool(s["tensor_filter"]),
+                 "tensor_items": s["tensor_items"], "of_items": s["n_tiles"], "band_pairs": s["band_pairs"],
+                 "count_pairs": s["count_pairs"], "identical_cluster_ids": bool(np.array_equal(ids, ref[0]))}
+            if full:
+                f["identical_counts"] = bool(np.array_equal(nn.cpu().numpy(), ref[1]))
+            forms[name] = f
+        ex, tf, ch = forms["exact_fp32_count"], forms["tensor_filter_count"], forms["chosen"]
+        forms["tensor_over_exact"] = ex["ms_per_step"] / tf["ms_per_step"]
+        forms["tensor_over_exact_count_kernel"] = ex["count_kernel_ms"] / tf["count_kernel_ms"]
+        forms["chosen_over_plain"] = ex["ms_per_step"] / ch["ms_per_step"]
+        # the audit: every pair the filter classified, against FP64 and the exact predicate
+        ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(), full_count=full,
+                       tensor_filter=True, audit=True)
+        torch.cuda.synchronize()
+        s = ctx.stats()
+        forms["filter_audit"] = {
+            "pairs": s["filter_audited_pairs"], "band_pairs": s["band_pairs"],
+            "band_fraction": s["band_pairs"] / max(s["filter_audited_pairs"], 1),
+            "max_abs_distance_error_vs_fp64": s["filter_max_abs_err"],
+            "max_error_over_guard_bound": s["filter_max_err_over_bound"],
+            "misclassified_pairs": s["filter_misclassified_pairs"],
+            "identical_cluster_ids": bool(np.array_equal(ci.cpu().numpy(), ref[0])),
+        }
+        out[mode] = forms
+    return out
+
+
 def run_ours(args):
     import importlib
 
-    import numpy as np
     import torch
 
     world, rank, local = dist_env()
@@ -289,14 +472,8 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     ctx = pkg.Context(local)
     ctx.set_stream(stream.cuda_stream)
-
-    x = torch.from_numpy(w.coords).cuda()
-    nn = torch.empty(n, dtype=torch.int32, device="cuda")
-    ci = torch.empty(n, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     full = args.full_count
-    torch.cuda.synchronize()
-
     ck_kw = {"exact": {"exact_count": True}, "tensor": {"tensor_filter": True}}.get(args.count_kernel, {})
     tuning = None
     if args.autotune and d >= 8 and not ck_kw:
@@ -305,132 +482,38 @@ def run_ours(args):
         tuning = {"best": r["best"],
                   "count_kernel_ms": {f"min_dim={c['tc_min_dim']},min_item={c['tc_min_item']}":
                                       round(c["ms_count_kernel"], 4) for c in r["table"]}}
-
-    def step():
-        return ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(), full_count=full,
-                              **ck_kw)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    barrier(world)
-    torch.cuda.synchronize()
-
-    step_ms, stats = [], []
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1)  # evict L2 between timed steps (not timed)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            res = step()
-            e1.record(stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            stats.append(ctx.stats())
-    torch.cuda.synchronize()
-    barrier(world)
-    value, total_ms = whole_job_rate(n, args.steps, sum(step_ms), world)
-
-    # d >= 8: the plain GPU form (exact FP32 count kernel) and the tensor-core filtered
-    # form beside the default (the library picks between them by tile fill)
-    forms = {}
-    if d >= 8 and not args.no_plain:
-        ci_chosen = ci.cpu().numpy()
-        for name, kw in (("exact_fp32_count", {"exact_count": True}), ("tensor_filter_count", {"tensor_filter": True})):
-            def form_step():
-                return ctx.run_device(x.data_ptr(), n, d, w.eps, w.min_pts, nn.data_ptr(), ci.data_ptr(),
-                                      full_count=full, **kw)
-            form_step()
-            torch.cuda.synchronize()
-            f_ms = []
-            for _ in range(args.steps):
-                flush.fill_(1)
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                form_step()
-                e1.record(stream)
-                e1.synchronize()
-                f_ms.append(e0.elapsed_time(e1))
-            fs = ctx.stats()
-            fv = n * len(f_ms) / (sum(f_ms) / 1000.0)
-            forms[name] = {"value": fv, "unit": UNIT, "ms_per_step": sum(f_ms) / len(f_ms),
-                           "count_kernel_ms": fs["ms_count_kernel"], "tensor_items": fs["tensor_items"],
-                           "band_pairs": fs["band_pairs"], "filtered_pairs": fs["count_pairs"],
-                           "identical_cluster_ids": bool(np.array_equal(ci.cpu().numpy(), ci_chosen))}
-        forms["chosen_over_plain"] = value / world / forms["exact_fp32_count"]["value"]
-
-    # end to end through the public API: pinned host input -> device -> pinned host labels
-    e2e = None
-    if not args.no_e2e:
-        hx = torch.from_numpy(w.coords).pin_memory()
-        hnn = torch.empty(n, dtype=torch.int32).pin_memory()
-        hci = torch.empty(n, dtype=torch.int32).pin_memory()
-        for _ in range(2):
-            ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
-                         full_count=full, **ck_kw)
-        torch.cuda.synchronize()
-        barrier(world)
-        e_ms = []
-        for _ in range(args.steps):
-            flush.fill_(1)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            ctx.run_ptrs(hx.data_ptr(), n, d, w.eps, w.min_pts, hnn.data_ptr(), hci.data_ptr(), device=False,
-                         full_count=full, **ck_kw)
-            e1.record(stream)
-            e1.synchronize()
-            e_ms.append(e0.elapsed_time(e1))
-        e_total = max_over_ranks(sum(e_ms), world)
-        e2e = {"value": world * n * args.steps / (e_total / 1000.0), "unit": UNIT,
-               "h2d_bytes_per_step": n * d * 4, "d2h_bytes_per_step": 2 * n * 4}
-
-    # roofline of the dominant kernel (device time measured with CUDA events inside the library)
-    hbm_peak, peak_src = peaks()
+    clk = ClockSampler(local)
+    m = measure_workload(pkg, ctx, w, args.steps, args.warmup, flush, stream, full, ck_kw, not args.no_e2e, world,
+                         clk)
     clk_sum = clk.summary()
-    kern = {
-        "count_kernel": statistics.mean(s["ms_count_kernel"] for s in stats),
-        "union_kernel": statistics.mean(s["ms_union_kernel"] for s in stats),
-        "border_kernel": statistics.mean(s["ms_border_kernel"] for s in stats),
-        "radix_sort": statistics.mean(s["ms_sort_kernels"] for s in stats),
-    }
+    stats = m["stats"]
     s0 = stats[-1]
-    dominant = max(kern, key=kern.get)
-    roof = roofline(dominant, kern[dominant], s0, n, hbm_peak, peak_src, clk_sum)
-    tkey = "tensor_count_kernel" if (dominant == "count_kernel" and s0["tensor_items"]) else dominant
-    roof["traffic"] = traffic_per_launch(w.name, tkey, n)
-    roof["traffic_source"] = "profiles/traffic_per_launch.md (ncu capture, scaled by n)" if roof["traffic"] else None
-
+    forms = None
+    if args.config == 3 and not args.no_plain and rank == 0:
+        forms = tensor_filter_forms(pkg, ctx, args.steps, flush, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(pkg, args.config, args.cpu_sample, os.cpu_count() or 1)
         cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
                                   "extrapolated_value_at_full_n", "full_n") if k in cb}
-
-    launches = count_launches(s0)
+    res = m["res"]
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator with the benchmark's distribution)",
             "config": {"workload": w.name, "n": n, "d": d, "eps": w.eps, "min_pts": w.min_pts,
                        "counts": "exact" if full else "early-exit at minPts (exact core flags and labels)",
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
-            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk_sum,
-            "gpu_launches": launches * args.steps, "count_forms": forms or None, "tuning": tuning,
+            "e2e": m.get("e2e"), "roofline": roofline_of(stats, n, w.name, clk_sum), "cpu_baseline": cpu,
+            "clocks": clk_sum, "gpu_launches": count_launches(s0) * args.steps, "count_forms": forms,
+            "tuning": tuning,
             "tensor_filter": {"used": bool(s0["tensor_filter"]), "items": s0["tensor_items"], "of_items": s0["n_tiles"],
                               "band_pairs": s0["band_pairs"]},
             "result": {"clusters": res.clusters, "noise": res.noise, "core_count": res.core_count},
-            "phases_ms": {k: round(statistics.mean(s[k] for s in stats), 4)
-                          for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
-            "kernels_ms": {k: round(v, 4) for k, v in kern.items()},
-            "pairs": {"count": s0["count_pairs"], "union": s0["union_pairs"], "border": s0["border_pairs"]},
-            "grid": {"cells": s0["n_cells"], "tiles": s0["n_tiles"], "rows": s0["stencil_rows"],
-                     "same_cell_linked": s0["same_cell_linked"], "key_bits": s0["key_bits"]},
+            **summary_of(stats),
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -456,7 +539,7 @@ def run_ours_batch(args):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     pkg = importlib.import_module("nextdbscan-exa_b200")
     lib = pkg.lib
     jobs = pkg.synthetic.config4(n_jobs=args.jobs)
@@ -495,29 +578,22 @@ def run_ours_batch(args):
                                                               "tensor": lib.FLAG_TENSOR_FILTER}.get(args.count_kernel, 0)
     dev_jobs = job_table(x.data_ptr(), nn.data_ptr(), ci.data_ptr())
     torch.cuda.synchronize()
+    stats = []
 
     def step():
         st = ctx.run_batched_jobs(dev_jobs, nj, lib.FLAG_DEVICE_PTRS | full)
         if st != 0:
             raise lib.NdbError(st, "ndb_b200_run_batched")
+        stats.append(ctx.stats())
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
-    step_ms, stats = [], []
+    stats.clear()
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            step()
-            e1.record(stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            stats.append(ctx.stats())
+        step_ms = timed(step, args.steps, flush, stream)
     torch.cuda.synchronize()
     barrier(world)
     value, total_ms = whole_job_rate(total, args.steps, sum(step_ms), world)
@@ -533,22 +609,13 @@ def run_ours_batch(args):
             for k, j in enumerate(jobs):
                 ctx.run_device(x.data_ptr() + 4 * int(foff[k]), j.n, j.d, j.eps, j.min_pts,
                                nn.data_ptr() + 4 * int(poff[k]), ci.data_ptr() + 4 * int(poff[k]),
-                               full_count=bool(full))
+                               full_count=bool(full & lib.FLAG_FULL_COUNT))
         plain_step()
         torch.cuda.synchronize()
-        p_ms = []
-        for _ in range(max(1, min(args.steps, 2))):
-            flush.fill_(1)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            plain_step()
-            e1.record(stream)
-            e1.synchronize()
-            p_ms.append(e0.elapsed_time(e1))
+        p_ms = timed(plain_step, max(1, min(args.steps, 3)), flush, stream)
         same = bool(np.array_equal(ci.cpu().numpy(), h_ci))
         pv = total * len(p_ms) / (sum(p_ms) / 1000.0)
-        plain = {"value": pv, "unit": UNIT, "ms_per_step": sum(p_ms) / len(p_ms),
+        plain = {"value": pv, "unit": UNIT, "ms_per_step": sum(p_ms) / len(p_ms), "steps": len(p_ms),
                  "form": "one ndb_b200_run call per job, device-resident inputs",
                  "chosen_over_plain": value / world / pv, "identical_cluster_ids": same}
 
@@ -567,33 +634,34 @@ def run_ours_batch(args):
         e2e_step()
         torch.cuda.synchronize()
         barrier(world)
-        e_ms = []
-        for _ in range(args.steps):
-            flush.fill_(1)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            e2e_step()
-            e1.record(stream)
-            e1.synchronize()
-            e_ms.append(e0.elapsed_time(e1))
+        e_ms = timed(e2e_step, args.steps, flush, stream)
         e_total = max_over_ranks(sum(e_ms), world)
         assert np.array_equal(hci.numpy(), h_ci), "host-buffer batch differs from the device-buffer batch"
         e2e = {"value": world * total * args.steps / (e_total / 1000.0), "unit": UNIT,
                "h2d_bytes_per_step": int(flat.nbytes), "d2h_bytes_per_step": 2 * total * 4}
 
-    hbm_peak, peak_src = peaks()
     clk_sum = clk.summary()
-    kern = {
-        "count_kernel": statistics.mean(s["ms_count_kernel"] for s in stats),
-        "union_kernel": statistics.mean(s["ms_union_kernel"] for s in stats),
-        "border_kernel": statistics.mean(s["ms_border_kernel"] for s in stats),
-        "radix_sort": statistics.mean(s["ms_sort_kernels"] for s in stats),
-    }
-    s0 = stats[-1]
-    dominant = max(kern, key=kern.get)
-    roof = roofline(dominant, kern[dominant], s0, total, hbm_peak, peak_src, clk_sum)
+    roof = roofline_of(stats, total, "batched-4096-jobs", clk_sum)
     roof["note"] = "summed over the pipelines of one batched call (one per dimensionality)"
+    s0 = stats[-1]
+    launches = count_launches(s0) * args.steps
+
+    # the other chosen form and the plain path at scale, measured in the same run
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        del x, nn, ci
+        torch.cuda.empty_cache()
+        extras["tensor_filter_8d_2m"] = tensor_filter_forms(pkg, ctx, args.steps, flush, stream)
+        w2 = pkg.synthetic.config2()
+        m2 = measure_workload(pkg, ctx, w2, args.steps, args.warmup, flush, stream, False, {}, not args.no_e2e, 1)
+        extras["plain_3d_10m"] = {
+            "workload": w2.name, "n": w2.n, "d": w2.d, "eps": w2.eps, "min_pts": w2.min_pts,
+            "value": m2["value"], "unit": UNIT, "ms_per_step": m2["ms_per_step"], "e2e": m2.get("e2e"),
+            "roofline": roofline_of(m2["stats"], w2.n, w2.name, clk_sum),
+            "result": {"clusters": m2["res"].clusters, "noise": m2["res"].noise, "core_count": m2["res"].core_count},
+            **summary_of(m2["stats"]),
+        }
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference_batch(pkg, os.cpu_count() or 1)
@@ -605,24 +673,22 @@ def run_ours_batch(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator with the benchmark's distribution)",
-            "config": {"workload": "batched-4096-jobs" if nj == 4096 else f"batched-subset-{nj}-jobs",
+            "config": {"workload": "batched-4096-jobs" if nj == BATCH_JOBS else f"batched-subset-{nj}-jobs",
                        "jobs": nj, "points": total,
                        "points_by_d": {int(d): int(sizes[dims == d].sum()) for d in np.unique(dims)},
                        "eps": "per job: 90th percentile of the 4-NN distance over a 1% sample",
                        "min_pts": "2d", "form": "ndb_b200_run_batched, device-resident inputs",
-                       "counts": "exact" if full else "early-exit at minPts (exact core flags and labels)",
+                       "counts": "exact" if args.full_count else "early-exit at minPts (exact core flags and labels)",
                        "l2": "flushed between timed steps (256 MB write); inputs 4.4 GB",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "e2e": e2e, "plain_gpu_form": plain, "roofline": roof, "cpu_baseline": cpu, "clocks": clk_sum,
-            "gpu_launches": count_launches(s0) * args.steps,
+            "gpu_launches": launches,
             "result": {"clusters": clusters, "noise": noise, "core_count": cores},
-            "phases_ms": {k: round(statistics.mean(s[k] for s in stats), 4)
-                          for k in ("ms_grid", "ms_count", "ms_union", "ms_border")},
-            "kernels_ms": {k: round(v, 4) for k, v in kern.items()},
             "pipelines": s0["pipelines"], "solo_jobs": s0["solo_jobs"],
             "tensor_filter": {"used": bool(s0["tensor_filter"]), "items": s0["tensor_items"], "of_items": s0["n_tiles"],
                               "band_pairs": s0["band_pairs"]},
-            "pairs": {"count": s0["count_pairs"], "union": s0["union_pairs"], "border": s0["border_pairs"]},
+            **summary_of(stats),
+            **extras,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -648,7 +714,7 @@ def traffic_per_launch(workload: str, kernel: str, n: int):
 
 
 def count_launches(s) -> int:
-    """Kernels of one job, as counted by the library at every launch site."""
+    """Kernels of one step, as counted by the library at every launch site."""
     return int(s["kernel_launches"])
 
 

@@ -75,6 +75,9 @@ typedef enum ndb_status {
                                     * filter (results are identical either way; this is the plain form) */
 #define NDB_FLAG_TENSOR_FILTER 0x10u /* d >= 8: count on the tensor-core filter whenever the input allows
                                       * it, whatever the tile-fill heuristic would pick (results identical) */
+#define NDB_FLAG_FILTER_AUDIT 0x20u  /* diagnostic: when the tensor-core filter runs, measure every pair it
+                                      * classifies against its FP64 distance and the exact FP32 predicate
+                                      * (ndb_stats.filter_*); slower, results identical */
 
 /* Mirrors nextdbscan::result (nextdbscan.h:43-48). */
 typedef struct ndb_result {
@@ -109,13 +112,21 @@ typedef struct ndb_stats {
     int32_t key_bytes;        /* 4 or 8 */
     int32_t kernel_launches;  /* kernels launched by the last classify + assign_labels */
     int32_t pipelines;        /* batched runs: pipelines built (one per d and chunk of jobs) */
-    int64_t count_pair_dims;  /* sum over pipelines of count_pairs x d (3 FP32 operations each) */
+    int64_t count_pair_dims;  /* dimensions evaluated by the count, summed over pipelines (3 FP32 operations each) */
     int64_t union_pair_dims;  /* the same for the union-find */
     int64_t border_pair_dims; /* the same for the border assignment */
     int32_t solo_jobs;        /* batched runs: jobs the pipelines could not take, run one call each */
     int32_t tensor_filter;    /* 1 when the neighbour count ran on the tensor-core filter (d >= 8) */
     int64_t band_pairs;       /* pairs inside the filter's guard band, rechecked with the exact predicate */
     int64_t tensor_items;     /* items (points of one cell, up to 32) counted on the tensor-core filter */
+    /* NDB_FLAG_FILTER_AUDIT only (0 otherwise): the filter's squared distance D~ against the FP64
+     * distance of the same FP32 points, over every pair it classified */
+    double filter_max_abs_err;        /* largest |D~ - d64| */
+    double filter_max_err_over_bound; /* largest |D~ - d64| over the error bound the guard band is built from */
+    int64_t filter_audited_pairs;     /* pairs measured */
+    int64_t filter_misclassified_pairs; /* pairs decided outside the band that the exact predicate decides otherwise */
+    int64_t count_skipped_dims;       /* pair dimensions the exact count never evaluated (d >= 8: a warp whose
+                                       * partial sums all passed eps^2 skips the rest; count_pair_dims excludes them) */
 } ndb_stats;
 
 typedef struct ndb_ctx ndb_ctx;
@@ -172,6 +183,19 @@ typedef struct ndb_job {
  * in the reference, which clusters one input per process (nextdbscan.cpp:28-68).
  * Returns the first failing job's status (each job also carries its own). */
 ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t n_jobs, uint32_t flags);
+
+/* The border pass of the last run again, with the caller's cluster ids for the core
+ * points: core_ids (n int32, input order; read for core points only) replaces the
+ * library's ids, every non-core point takes the minimum of those ids over the cores
+ * within eps (the reference's tie rule, data_process.cpp:204-209), and
+ * cluster_index_out (n int32, may be NULL) receives the result in input order.
+ * Host or device pointers as the run's NDB_FLAG_DEVICE_PTRS says.  The cores of one
+ * component must carry one id.  For the sharded form: there a component spans ranks,
+ * its final id is known only after the ranks' merge, and a border point's minimum
+ * over the local ids would not survive that merge -- the step that replaces the
+ * reference's allreduce-min of labels across ranks (data_process.cpp:232-233).
+ * Afterwards ndb_b200_cluster_label returns NDB_ERR_NO_STATE. */
+ndb_status ndb_b200_assign_border(ndb_ctx *ctx, const int32_t *core_ids, int32_t *cluster_index_out);
 
 /* Per-core label array of the last run, the reference's v_cluster_label
  * (data_process.h:58, filled at data_process.cpp:141-260): entry k is the cluster id

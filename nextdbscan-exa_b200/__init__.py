@@ -51,10 +51,10 @@ def _as_points(v_coord, n_dim: int | None = None) -> np.ndarray:
 
 
 def _flags(full_count: bool, approximate: bool, exact_count: bool = False, tensor_filter: bool = False,
-           device: bool = False) -> int:
+           device: bool = False, audit: bool = False) -> int:
     return ((lib.FLAG_FULL_COUNT if full_count else 0) | (lib.FLAG_APPROXIMATE if approximate else 0)
             | (lib.FLAG_EXACT_COUNT if exact_count else 0) | (lib.FLAG_TENSOR_FILTER if tensor_filter else 0)
-            | (lib.FLAG_DEVICE_PTRS if device else 0))
+            | (lib.FLAG_DEVICE_PTRS if device else 0) | (lib.FLAG_FILTER_AUDIT if audit else 0))
 
 
 class Context:
@@ -117,11 +117,11 @@ class Context:
         return ci, Result(res.clusters, res.noise, res.core_count, res.n)
 
     def run(self, coords, eps: float, min_pts: int, *, full_count: bool = False,
-            approximate: bool = False, exact_count: bool = False,
-            tensor_filter: bool = False) -> tuple[np.ndarray, np.ndarray, Result]:
+            approximate: bool = False, exact_count: bool = False, tensor_filter: bool = False,
+            audit: bool = False) -> tuple[np.ndarray, np.ndarray, Result]:
         pts = _as_points(coords)
         n, d = pts.shape
-        flags = _flags(full_count, approximate, exact_count, tensor_filter)
+        flags = _flags(full_count, approximate, exact_count, tensor_filter, audit=audit)
         nn = np.empty(n, dtype=np.int32)
         ci = np.empty(n, dtype=np.int32)
         res = lib.NdbResult()
@@ -134,9 +134,9 @@ class Context:
     # -- raw addresses: host (pageable or pinned) or, with device=True, device memory --
     def run_ptrs(self, coords_ptr: int, n: int, d: int, eps: float, min_pts: int, nn_ptr: int | None,
                  ci_ptr: int | None, *, device: bool, full_count: bool = False,
-                 approximate: bool = False, exact_count: bool = False,
-            tensor_filter: bool = False) -> Result:
-        flags = _flags(full_count, approximate, exact_count, tensor_filter, device)
+                 approximate: bool = False, exact_count: bool = False, tensor_filter: bool = False,
+                 audit: bool = False) -> Result:
+        flags = _flags(full_count, approximate, exact_count, tensor_filter, device, audit)
         res = lib.NdbResult()
         st = self._lib.ndb_b200_run(self._h, ctypes.c_void_p(coords_ptr), n, d, ctypes.c_float(eps),
                                     int(min_pts), flags, ctypes.c_void_p(nn_ptr or 0),
@@ -148,8 +148,8 @@ class Context:
     # -- device buffers (addresses of device memory, e.g. torch tensors) ---
     def run_device(self, coords_ptr: int, n: int, d: int, eps: float, min_pts: int, nn_ptr: int | None,
                    ci_ptr: int | None, *, full_count: bool = False, approximate: bool = False,
-                   exact_count: bool = False, tensor_filter: bool = False) -> Result:
-        flags = _flags(full_count, approximate, exact_count, tensor_filter, True)
+                   exact_count: bool = False, tensor_filter: bool = False, audit: bool = False) -> Result:
+        flags = _flags(full_count, approximate, exact_count, tensor_filter, True, audit)
         res = lib.NdbResult()
         st = self._lib.ndb_b200_run(self._h, ctypes.c_void_p(coords_ptr), n, d, ctypes.c_float(eps),
                                     int(min_pts), flags, ctypes.c_void_p(nn_ptr or 0),
@@ -189,6 +189,18 @@ class Context:
         """Raw form: jobs is a ctypes array of lib.NdbJob (addresses filled by the
         caller, host or device per flags).  Returns the status without raising."""
         return self._lib.ndb_b200_run_batched(self._h, jobs, int(n_jobs), int(flags))
+
+    def assign_border(self, core_ids) -> np.ndarray:
+        """The border pass of the last run (host buffers) again with the caller's ids
+        for the core points (n int32, input order); returns every point's cluster
+        index.  See ndb_b200_assign_border."""
+        ids = np.ascontiguousarray(np.asarray(core_ids, dtype=np.int32))
+        if ids.shape != (self.n,):
+            raise ValueError("core_ids must hold one int32 per point of the last run")
+        out = np.empty(self.n, dtype=np.int32)
+        st = self._lib.ndb_b200_assign_border(self._h, ids.ctypes.data, out.ctypes.data)
+        lib.check(st, "ndb_b200_assign_border", self._h)
+        return out
 
     def cluster_label(self, core_count: int) -> np.ndarray:
         out = np.empty(max(core_count, 0), dtype=np.int32)

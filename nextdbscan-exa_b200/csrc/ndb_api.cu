@@ -37,6 +37,10 @@ struct ndb_ctx {
     DevBuf nn_sorted, nn_orig, core_sorted, core_bits, core_prefix, ci_sorted, ci_orig, labels;
     // per-cell arrays
     DevBuf cell_start, cell_key, nbr, item_cnt, items, cell_has_core, cell_cid, hash_keys, hash_vals;
+    // column table of the grid (CellIndex): one [first, end) cell range per column
+    DevBuf col_range;
+    size_t col_budget = size_t(1) << 27;  // largest column table (entries) a run may build, else the hash table
+    bool use_cols = false;                // the current job's cells are found through the column table
     // union-find
     DevBuf parent, comp_min;
     // neighbour lists of the points whose count stays below min_pts (border step)
@@ -51,6 +55,8 @@ struct ndb_ctx {
     DevBuf jobs_dev, batch_bbox, cell_job, job_counters;
     // items split between the tensor-core count (full items) and the exact one
     DevBuf items_split;
+    // caller's core ids of ndb_b200_assign_border (host inputs)
+    DevBuf ids_in;
     // largest device footprint the context may hold (bytes); 0 = no cap
     size_t mem_limit = 0;
     // count-kernel thresholds set by ndb_b200_set_tuning (0: the library's defaults)
@@ -66,7 +72,7 @@ struct ndb_ctx {
                           &cell_key,    &nbr,         &item_cnt,    &items,       &cell_has_core, &cell_cid,
                           &parent,      &comp_min,    &sort_hist,   &scan_scratch, &small,      &hash_keys,
                           &hash_vals,   &nbr_list,    &jobs_dev,    &batch_bbox,  &cell_job,    &job_counters,
-                          &items_split};
+                          &items_split, &col_range,   &ids_in};
         for (DevBuf *b : bufs) f(*b);
     }
     size_t held_bytes() {
@@ -105,8 +111,11 @@ namespace {
 // layout of ctx->small
 constexpr size_t kSmallBboxOff = 0;          // int[2*kMaxDim]
 constexpr size_t kSmallInvalidOff = 256;     // u64
-constexpr size_t kSmallCountersOff = 512;    // u64[8]: 0 clusters 1 noise 2 count pairs 3 union pairs 4 border pairs
+constexpr size_t kSmallCountersOff = 512;    // u64[12]: 0 clusters 1 noise 2 count pairs 3 union pairs 4 border pairs
                                              // 5 band pairs 6 work counter of the persistent count kernel
+                                             // 7 pair dimensions the count skipped (partial sums past e2)
+                                             // 8..11 filter audit (tc::audit_tile)
+constexpr int kCounters = 12;
 constexpr size_t kSmallScalarOff = 1024;     // u32[8]: 0 n_cells 1 n_items 2 n_cores
 constexpr size_t kSmallErrOff = 1536;        // int
 constexpr size_t kSmallStencilOff = 2048;    // int4[kMaxRows]: stencil rows of the current job
@@ -124,6 +133,9 @@ inline unsigned blocks_for(int64_t n, int threads = kBlock) {
 struct Fail {
     ndb_status st;
 };
+
+constexpr uint32_t kAllFlags = NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS |
+                               NDB_FLAG_EXACT_COUNT | NDB_FLAG_TENSOR_FILTER | NDB_FLAG_FILTER_AUDIT;
 
 inline void ck(ndb_ctx *ctx, cudaError_t e) {
     if (e == cudaSuccess) return;
@@ -300,6 +312,54 @@ inline int row_group_log2(int n_rows) {
     return l;
 }
 
+// Columns of a grid: cells that differ only in gridded dimension 0.
+inline double grid_columns(const GridDev &g) {
+    double c = 1;
+    for (int a = 1; a < g.k; ++a) c *= (double)g.g[a];
+    return c;
+}
+
+// The cell lookup of a pipeline: the dense column table when the columns of all
+// its jobs fit the context's budget, else a hash table of the cell keys (load
+// factor <= 1/4, so most probes settle at the first slot).
+template <typename K>
+CellIndex<K> build_cell_index(ndb_ctx *ctx, int64_t n_cells, double columns, const GridDev &g_one,
+                              const JobDev *jobs, const int32_t *cell_job) {
+    cudaStream_t st = ctx->stream;
+    CellIndex<K> L{nullptr, nullptr, nullptr, 0};
+    ctx->use_cols = columns >= 1 && columns <= (double)ctx->col_budget;
+    if (ctx->use_cols) {
+        const size_t cols = (size_t)columns;
+        ensure(ctx, ctx->col_range, (cols + 1) * sizeof(int2));
+        ck(ctx, cudaMemsetAsync(ctx->col_range.ptr, 0, (cols + 1) * sizeof(int2), st));
+        ++launch_counter(), col_range_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
+            ctx->cell_key.as<K>(), n_cells, g_one, jobs, cell_job, ctx->col_range.as<int2>());
+        ck(ctx, cudaGetLastError());
+        L.col = ctx->col_range.as<int2>();
+        return L;
+    }
+    int64_t hsize = 1024;
+    while (hsize < 4 * n_cells) hsize <<= 1;
+    ctx->hash_mask = (unsigned long long)(hsize - 1);
+    ensure(ctx, ctx->hash_keys, hsize * sizeof(K));
+    ensure(ctx, ctx->hash_vals, hsize * sizeof(int32_t));
+    ++launch_counter(), hash_clear_kernel<K><<<blocks_for(hsize), kBlock, 0, st>>>(ctx->hash_keys.as<K>(), hsize);
+    ++launch_counter(), hash_insert_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
+        ctx->cell_key.as<K>(), n_cells, ctx->hash_keys.as<K>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask);
+    ck(ctx, cudaGetLastError());
+    L.hkeys = ctx->hash_keys.as<K>();
+    L.hvals = ctx->hash_vals.as<int32_t>();
+    L.mask = ctx->hash_mask;
+    return L;
+}
+
+// The lookup built by build_cell_index, for kernels of the label phase.
+template <typename K>
+CellIndex<K> cell_index(ndb_ctx *ctx) {
+    if (ctx->use_cols) return CellIndex<K>{ctx->col_range.as<int2>(), nullptr, nullptr, 0};
+    return CellIndex<K>{nullptr, ctx->hash_keys.as<K>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask};
+}
+
 template <int D, typename K>
 void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     cudaStream_t st = ctx->stream;
@@ -365,24 +425,15 @@ void classify_grid(ndb_ctx *ctx, const Plan &pl) {
     const int64_t n_cells = n_cells32;
     ctx->n_cells = n_cells;
 
-    // neighbour rows, through a hash table of the cells
+    // neighbour rows, through the column table (or a hash table) of the cells
     const int n_rows = pl.st.n_rows;
-    int64_t hsize = 1024;
-    while (hsize < 4 * n_cells) hsize <<= 1;  // load factor <= 1/4: most probes settle at the first slot
-    ctx->hash_mask = (unsigned long long)(hsize - 1);
-    ensure(ctx, ctx->hash_keys, hsize * sizeof(K));
-    ensure(ctx, ctx->hash_vals, hsize * sizeof(int32_t));
-    ++launch_counter(), hash_clear_kernel<K><<<blocks_for(hsize), kBlock, 0, st>>>(ctx->hash_keys.as<K>(), hsize);
-    ++launch_counter(), hash_insert_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
-        ctx->cell_key.as<K>(), n_cells, ctx->hash_keys.as<K>(), ctx->hash_vals.as<int32_t>(),
-        (unsigned long long)(hsize - 1));
+    const CellIndex<K> L = build_cell_index<K>(ctx, n_cells, grid_columns(pl.g), pl.g, nullptr, nullptr);
     ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
     int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
     ck(ctx, cudaMemcpyAsync(rows_dev, pl.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
     const int rlog = row_group_log2(n_rows);
     ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells << rlog), kBlock, 0, st>>>(
-        ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, rlog, ctx->hash_keys.as<K>(),
-        ctx->hash_vals.as<int32_t>(), (unsigned long long)(hsize - 1), ctx->nbr.as<int2>(), nullptr, nullptr);
+        ctx->cell_key.as<K>(), n_cells, pl.g, rows_dev, n_rows, rlog, L, ctx->nbr.as<int2>(), nullptr, nullptr);
     ck(ctx, cudaGetLastError());
 
     // work items
@@ -461,17 +512,23 @@ template <int D>
 void launch_count_tc(ndb_ctx *ctx, int64_t n_items, const int2 *items, const int32_t *cell_start, const int2 *nbr,
                      int n_rows, const float *xs, float e2, int min_pts, bool early, int32_t *nn_sorted,
                      int32_t *list, int list_cap, int list_stride, const JobDev *jobs, const int32_t *cell_job,
-                     const uint32_t *n_items_dev) {
+                     const uint32_t *n_items_dev, bool audit) {
     if constexpr (D >= tc::kMinDim) {
         cudaStream_t st = ctx->stream;
         unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
         unsigned int *work = reinterpret_cast<unsigned int *>(counters + 6);
         ck(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
         const unsigned grid = (unsigned)std::min<int64_t>(n_items, (int64_t)ctx->sm_count * 4);
-        ++launch_counter(), tc::count_tc_kernel<D><<<grid, tc::kThreads, 0, st>>>(
-            items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, early ? 1 : 0, nn_sorted, list, list_cap,
-            list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job,
-            n_items_dev);
+        if (audit)
+            ++launch_counter(), tc::count_tc_kernel<D, true><<<grid, tc::kThreads, 0, st>>>(
+                items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, early ? 1 : 0, nn_sorted, list, list_cap,
+                list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job,
+                n_items_dev, counters + 8);
+        else
+            ++launch_counter(), tc::count_tc_kernel<D><<<grid, tc::kThreads, 0, st>>>(
+                items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, early ? 1 : 0, nn_sorted, list, list_cap,
+                list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job,
+                n_items_dev);
         ck(ctx, cudaGetLastError());
     } else {
         throw Fail{NDB_ERR_INVALID_ARGUMENT};
@@ -485,7 +542,7 @@ template <int D>
 void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_items, const int2 *items,
                  const int32_t *cell_start, const int2 *nbr, int n_rows, const float *xs, float e2, int min_pts,
                  int dense_skip, int32_t *nn_sorted, int32_t *list, int list_cap, int list_stride,
-                 const JobDev *jobs, const int32_t *cell_job) {
+                 const JobDev *jobs, const int32_t *cell_job, bool audit) {
     if (n_items <= 0) return;
     cudaStream_t st = ctx->stream;
     unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
@@ -501,7 +558,7 @@ void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_ite
             items, n_items, cell_start, force_tc ? 1 : ctx_tc_min_item(ctx), tc_items, scal + 4, rest, scal + 5);
         ck(ctx, cudaGetLastError());
         launch_count_tc<D>(ctx, n_items, tc_items, cell_start, nbr, n_rows, xs, e2, min_pts, early, nn_sorted, list,
-                           list_cap, list_stride, jobs, cell_job, scal + 4);
+                           list_cap, list_stride, jobs, cell_job, scal + 4, audit);
         ex_items = rest;
         ex_n = scal + 5;
     }
@@ -509,11 +566,11 @@ void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_ite
     if (early)
         ++launch_counter(), count_kernel<D, true><<<grid, kCountWarps * kWarp, 0, st>>>(
             ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
-            list_stride, counters + 2, jobs, cell_job, ex_n);
+            list_stride, counters + 2, jobs, cell_job, ex_n, counters + 7);
     else
         ++launch_counter(), count_kernel<D, false><<<grid, kCountWarps * kWarp, 0, st>>>(
             ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
-            list_stride, counters + 2, jobs, cell_job, ex_n);
+            list_stride, counters + 2, jobs, cell_job, ex_n, counters + 7);
     ck(ctx, cudaGetLastError());
 }
 
@@ -535,7 +592,7 @@ void count_phase(ndb_ctx *ctx) {
     count_items<D>(ctx, ctx->tc_count, (ctx->flags_run & NDB_FLAG_TENSOR_FILTER) != 0, early, ctx->n_items,
                    ctx->items.as<int2>(), ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                    ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
-                   ctx->list_cap, ctx->list_cap, nullptr, nullptr);
+                   ctx->list_cap, ctx->list_cap, nullptr, nullptr, (ctx->flags_run & NDB_FLAG_FILTER_AUDIT) != 0);
     cudaEventRecord(ctx->kev[3], st);
 }
 
@@ -580,6 +637,30 @@ void classify_dispatch(ndb_ctx *ctx, const Plan &pl) {
 // ---------------------------------------------------------------------------
 // phase 2
 // ---------------------------------------------------------------------------
+// Border points: the minimum id over the cores in range, from the count's
+// neighbour lists when there are lists, else by a stencil scan.  Reads the core ids
+// in ci_sorted (point units) or cell_cid (cell units).
+template <int D>
+void border_phase(ndb_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    const int64_t nv = ctx->nv;
+    unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
+    if (ctx->list_cap > 0) {
+        ++launch_counter(), border_list_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+            nv, ctx->nn_sorted.as<int32_t>(), ctx->nbr_list.as<int32_t>(), ctx->list_cap,
+            ctx->core_sorted.as<uint8_t>(), ctx->cell_units, ctx->pcell.as<int32_t>(), ctx->cell_cid.as<int32_t>(),
+            ctx->ci_sorted.as<int32_t>(), counters + 4);
+        ck(ctx, cudaGetLastError());
+    } else if (ctx->n_items > 0) {
+        const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
+        ++launch_counter(), border_kernel<D><<<grid, kBlock, 0, st>>>(
+            ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
+            ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
+            ctx->cell_units, ctx->cell_cid.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters + 4);
+        ck(ctx, cudaGetLastError());
+    }
+}
+
 template <int D>
 void labels_phase(ndb_ctx *ctx) {
     cudaStream_t st = ctx->stream;
@@ -597,20 +678,19 @@ void labels_phase(ndb_ctx *ctx) {
     ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units, kNoCluster);
     ck(ctx, cudaGetLastError());
 
-    const unsigned grid = (unsigned)((ctx->n_items + kWarpsPerBlock - 1) / kWarpsPerBlock);
     cudaEventRecord(ctx->kev[4], st);  // moved to the main union kernel below when there is one
     if (ctx->n_items > 0) {
         if (ctx->cell_units) {
             if (ctx->key64)
                 ++launch_counter(), union_near_kernel<D, uint64_t><<<blocks_for(n_cells), kBlock, 0, st>>>(
                     n_cells, ctx->grid, ctx->cell_key.as<uint64_t>(), ctx->cell_start.as<int32_t>(),
-                    ctx->hash_keys.as<uint64_t>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask, ctx->xs.as<float>(),
+                    cell_index<uint64_t>(ctx), ctx->xs.as<float>(),
                     ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
                     ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
             else
                 ++launch_counter(), union_near_kernel<D, uint32_t><<<blocks_for(n_cells), kBlock, 0, st>>>(
                     n_cells, ctx->grid, ctx->cell_key.as<uint32_t>(), ctx->cell_start.as<int32_t>(),
-                    ctx->hash_keys.as<uint32_t>(), ctx->hash_vals.as<int32_t>(), ctx->hash_mask, ctx->xs.as<float>(),
+                    cell_index<uint32_t>(ctx), ctx->xs.as<float>(),
                     ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
                     ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
             ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
@@ -664,19 +744,7 @@ void labels_phase(ndb_ctx *ctx) {
     ck(ctx, cudaGetLastError());
     cudaEventRecord(ctx->ev[3], st);
     cudaEventRecord(ctx->kev[6], st);
-    if (ctx->list_cap > 0) {
-        ++launch_counter(), border_list_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
-            nv, ctx->nn_sorted.as<int32_t>(), ctx->nbr_list.as<int32_t>(), ctx->list_cap,
-            ctx->core_sorted.as<uint8_t>(), ctx->cell_units, ctx->pcell.as<int32_t>(), ctx->cell_cid.as<int32_t>(),
-            ctx->ci_sorted.as<int32_t>(), counters + 4);
-        ck(ctx, cudaGetLastError());
-    } else if (ctx->n_items > 0) {
-        ++launch_counter(), border_kernel<D><<<grid, kBlock, 0, st>>>(
-            ctx->items.as<int2>(), ctx->n_items, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
-            ctx->xs.as<float>(), ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
-            ctx->cell_units, ctx->cell_cid.as<int32_t>(), ctx->ci_sorted.as<int32_t>(), counters + 4);
-        ck(ctx, cudaGetLastError());
-    }
+    border_phase<D>(ctx);
     cudaEventRecord(ctx->kev[7], st);
     // ids in input order, straight into the caller's device buffer when there is one
     int32_t *target = nullptr;
@@ -711,10 +779,21 @@ bool is_device_ptr(const void *p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// The filter audit's counters (tc::audit_tile) into the stats.
+inline void audit_stats(ndb_stats &S, const unsigned long long *a) {
+    double mx, mr;
+    memcpy(&mx, &a[0], sizeof(double));
+    memcpy(&mr, &a[1], sizeof(double));
+    S.filter_max_abs_err = mx;
+    S.filter_max_err_over_bound = mr;
+    S.filter_audited_pairs = (int64_t)a[2];
+    S.filter_misclassified_pairs = (int64_t)a[3];
+}
+
 // Counters and times of phase 1, once its work on the context's stream is done.
 template <int D>
 void classify_stats(ndb_ctx *ctx) {
-    unsigned long long h_counters[8];
+    unsigned long long h_counters[kCounters];
     uint32_t h_tc_items = 0;
     ck(ctx, cudaMemcpyAsync(h_counters, small_at<unsigned long long>(ctx, kSmallCountersOff), sizeof(h_counters),
                             cudaMemcpyDeviceToHost, ctx->stream));
@@ -723,8 +802,10 @@ void classify_stats(ndb_ctx *ctx) {
     ck(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->stats.tensor_items = ctx->tc_count ? h_tc_items : 0;
     ctx->stats.count_pairs = (int64_t)h_counters[2];
-    ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
+    ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D - (int64_t)h_counters[7];
+    ctx->stats.count_skipped_dims = (int64_t)h_counters[7];
     ctx->stats.band_pairs = (int64_t)h_counters[5];
+    audit_stats(ctx->stats, h_counters + 8);
     ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
     ctx->stats.ms_count = elapsed(ctx->ev[1], ctx->ev[2]);
     ctx->stats.ms_sort_kernels = elapsed(ctx->kev[0], ctx->kev[1]);
@@ -847,7 +928,7 @@ ndb_status labels_impl(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
     const int64_t n = ctx->n;
     if (ci_out && !(ctx->flags_run & NDB_FLAG_DEVICE_PTRS))
         ck(ctx, cudaMemcpyAsync(ci_out, ctx->ci_orig.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    unsigned long long h_counters[8];
+    unsigned long long h_counters[kCounters];
     uint32_t h_scal[8];
     int h_err = 0;
     ck(ctx, cudaMemcpyAsync(h_counters, small_at<unsigned long long>(ctx, kSmallCountersOff), sizeof(h_counters),
@@ -862,8 +943,10 @@ ndb_status labels_impl(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
         ctx->stats_pending = false;
         ctx->stats.tensor_items = ctx->tc_count ? h_scal[4] : 0;
         ctx->stats.count_pairs = (int64_t)h_counters[2];
-        ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
+        ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D - (int64_t)h_counters[7];
+        ctx->stats.count_skipped_dims = (int64_t)h_counters[7];
         ctx->stats.band_pairs = (int64_t)h_counters[5];
+        audit_stats(ctx->stats, h_counters + 8);
         ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
         ctx->stats.ms_count = elapsed(ctx->ev[1], ctx->ev[2]);
         ctx->stats.ms_sort_kernels = elapsed(ctx->kev[0], ctx->kev[1]);
@@ -904,6 +987,47 @@ template <int D>
 ndb_status labels_entry(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
     try {
         return labels_impl<D>(ctx, ci_out, result);
+    } catch (const Fail &f) {
+        return f.st;
+    }
+}
+
+// ndb_b200_assign_border: the border pass again, with the caller's ids for the cores.
+template <int D>
+ndb_status border_ids_impl(ndb_ctx *ctx, const int32_t *core_ids, int32_t *ci_out) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = ctx->n, nv = ctx->nv;
+    const bool dev = (ctx->flags_run & NDB_FLAG_DEVICE_PTRS) != 0;
+    const int32_t *ids = core_ids;
+    if (!dev) {
+        ensure(ctx, ctx->ids_in, (size_t)(n + 1) * sizeof(int32_t));
+        ck(ctx, cudaMemcpyAsync(ctx->ids_in.ptr, core_ids, n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        ids = ctx->ids_in.as<int32_t>();
+    }
+    ++launch_counter(), set_core_ids_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+        nv, ctx->core_sorted.as<uint8_t>(), ctx->ids0.as<int32_t>(), ids, ctx->pcell.as<int32_t>(), ctx->cell_units,
+        ctx->ci_sorted.as<int32_t>(), ctx->cell_cid.as<int32_t>());
+    ck(ctx, cudaGetLastError());
+    border_phase<D>(ctx);
+    if (ci_out) {
+        int32_t *target = ci_out;
+        if (!dev) {
+            ensure(ctx, ctx->ci_orig, (n + 1) * sizeof(int32_t));
+            target = ctx->ci_orig.as<int32_t>();
+        }
+        ++launch_counter(), output_ids_kernel<<<blocks_for(n), kBlock, 0, st>>>(
+            ctx->ci_sorted.as<int32_t>(), nv, n, ctx->ids0.as<int32_t>(), ctx->core_bits.as<uint32_t>(), ids, target);
+        ck(ctx, cudaGetLastError());
+        if (!dev) ck(ctx, cudaMemcpyAsync(ci_out, target, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    }
+    ck(ctx, cudaStreamSynchronize(st));
+    return NDB_OK;
+}
+
+template <int D>
+ndb_status border_ids_entry(ndb_ctx *ctx, const int32_t *core_ids, int32_t *ci_out) {
+    try {
+        return border_ids_impl<D>(ctx, core_ids, ci_out);
     } catch (const Fail &f) {
         return f.st;
     }
@@ -1045,8 +1169,7 @@ ndb_status ndb_b200_classify(ndb_ctx *ctx, const float *coords, int64_t n, int32
                              uint32_t flags, int32_t *nn_out) {
     ndb_status s = check_ctx(ctx);
     if (s != NDB_OK) return s;
-    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS | NDB_FLAG_EXACT_COUNT |
-                  NDB_FLAG_TENSOR_FILTER)) return NDB_ERR_INVALID_ARGUMENT;
+    if (flags & ~kAllFlags) return NDB_ERR_INVALID_ARGUMENT;
     if (n < 0) return NDB_ERR_INVALID_ARGUMENT;
     if (n > NDB_MAX_POINTS) return NDB_ERR_TOO_MANY_POINTS;
     if (d < 1 || d > NDB_MAX_DIM) return NDB_ERR_UNSUPPORTED_DIM;
@@ -1128,6 +1251,23 @@ ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capa
     return NDB_OK;
 }
 
+ndb_status ndb_b200_assign_border(ndb_ctx *ctx, const int32_t *core_ids, int32_t *cluster_index_out) {
+    ndb_status s = check_ctx(ctx);
+    if (s != NDB_OK) return s;
+    if (!ctx->have_labels) return NDB_ERR_NO_STATE;
+    if (ctx->n == 0) return NDB_OK;
+    if (!core_ids) return NDB_ERR_INVALID_ARGUMENT;
+    if (ctx->flags_run & NDB_FLAG_DEVICE_PTRS) {
+        if (!is_device_ptr(core_ids) || (cluster_index_out && !is_device_ptr(cluster_index_out)))
+            return NDB_ERR_INVALID_ARGUMENT;
+    }
+    // the pass replaces the library's own ids: ndb_b200_cluster_label would now report the caller's
+    ctx->have_labels = false;
+#define NDB_BORDER(D) border_ids_entry<D>(ctx, core_ids, cluster_index_out)
+    NDB_DISPATCH_D(ctx->d, NDB_BORDER)
+#undef NDB_BORDER
+}
+
 ndb_status ndb_b200_get_stats(ndb_ctx *ctx, ndb_stats *stats) {
     if (!ctx || !stats) return NDB_ERR_INVALID_ARGUMENT;
     *stats = ctx->stats;
@@ -1172,6 +1312,7 @@ struct BatchPlan {
     int list_stride = 0;
     bool tc = false;  // neighbour count on the tensor-core filter (every job eligible)
     int64_t total_n = 0, nv = 0;
+    double columns = 0;  // entries of the pipeline's column table (sum over its jobs)
 };
 
 template <int D, typename K>
@@ -1246,23 +1387,16 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         ctx->cell_key.as<K>(), n_cells, jobs_dev, nj, ctx->cell_job.as<int32_t>());
     const int32_t *cell_job = ctx->cell_job.as<int32_t>();
 
-    // neighbour rows through the cell hash table
+    // neighbour rows through the column table (or the hash table) of the cells
     const int n_rows = bp.st.n_rows;
-    int64_t hsize = 1024;
-    while (hsize < 4 * n_cells) hsize <<= 1;
-    const unsigned long long hmask = (unsigned long long)(hsize - 1);
-    ensure(ctx, ctx->hash_keys, hsize * sizeof(K));
-    ensure(ctx, ctx->hash_vals, hsize * sizeof(int32_t));
-    ++launch_counter(), hash_clear_kernel<K><<<blocks_for(hsize), kBlock, 0, st>>>(ctx->hash_keys.as<K>(), hsize);
-    ++launch_counter(), hash_insert_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
-        ctx->cell_key.as<K>(), n_cells, ctx->hash_keys.as<K>(), ctx->hash_vals.as<int32_t>(), hmask);
+    const CellIndex<K> L = build_cell_index<K>(ctx, n_cells, (double)bp.columns, bp.jd[0].g, jobs_dev, cell_job);
     ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
     int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
     ck(ctx, cudaMemcpyAsync(rows_dev, bp.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
     const int rlog = row_group_log2(n_rows);
     ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells << rlog), kBlock, 0, st>>>(
-        ctx->cell_key.as<K>(), n_cells, bp.jd[0].g, rows_dev, n_rows, rlog, ctx->hash_keys.as<K>(),
-        ctx->hash_vals.as<int32_t>(), hmask, ctx->nbr.as<int2>(), jobs_dev, cell_job);
+        ctx->cell_key.as<K>(), n_cells, bp.jd[0].g, rows_dev, n_rows, rlog, L, ctx->nbr.as<int2>(), jobs_dev,
+        cell_job);
     ck(ctx, cudaGetLastError());
 
     // work items
@@ -1291,7 +1425,8 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     cudaEventRecord(ctx->kev[2], st);
     count_items<D>(ctx, bp.tc, (flags & NDB_FLAG_TENSOR_FILTER) != 0, early, n_items, ctx->items.as<int2>(),
                    ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows, ctx->xs.as<float>(), 0.0f, 0, 0,
-                   ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, jobs_dev, cell_job);
+                   ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, jobs_dev, cell_job,
+                   (flags & NDB_FLAG_FILTER_AUDIT) != 0);
     cudaEventRecord(ctx->kev[3], st);
     const int64_t n_words = (n + 31) / 32;
     ensure(ctx, ctx->core_sorted, n + 1);
@@ -1326,8 +1461,8 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     if (n_items > 0) {
         if (bp.linked) {
             ++launch_counter(), union_near_kernel<D, K><<<blocks_for(n_cells), kBlock, 0, st>>>(
-                n_cells, bp.jd[0].g, ctx->cell_key.as<K>(), ctx->cell_start.as<int32_t>(), ctx->hash_keys.as<K>(),
-                ctx->hash_vals.as<int32_t>(), hmask, ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(),
+                n_cells, bp.jd[0].g, ctx->cell_key.as<K>(), ctx->cell_start.as<int32_t>(), L,
+                ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(),
                 ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err, jobs_dev, cell_job);
             ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                       n_units, err);
@@ -1395,11 +1530,15 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     cudaEventRecord(ctx->ev[4], st);
     std::vector<unsigned long long> h_jc((size_t)4 * nj);
     unsigned long long h_pairs[4] = {0, 0, 0, 0};  // count, union, border, band pairs (running totals)
+    unsigned long long h_audit[4] = {0, 0, 0, 0};  // filter audit (running over the call's pipelines)
+    unsigned long long h_skipped = 0;              // pair dimensions the count skipped (running total)
     uint32_t h_tc_items = 0;
     int h_err = 0;
     if (bp.tc)
         ck(ctx, cudaMemcpyAsync(&h_tc_items, scal + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_pairs, counters + 2, sizeof(h_pairs), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaMemcpyAsync(h_audit, counters + 8, sizeof(h_audit), cudaMemcpyDeviceToHost, st));
+    ck(ctx, cudaMemcpyAsync(&h_skipped, counters + 7, sizeof(h_skipped), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_jc.data(), jc, (size_t)4 * nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             st));
     ck(ctx, cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1423,12 +1562,14 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     const int64_t dc = (int64_t)h_pairs[0] - S.count_pairs, du = (int64_t)h_pairs[1] - S.union_pairs,
                   db = (int64_t)h_pairs[2] - S.border_pairs;
     S.band_pairs = (int64_t)h_pairs[3];
+    audit_stats(S, h_audit);
     S.tensor_items += h_tc_items;
     S.tensor_filter |= bp.tc ? 1 : 0;
     S.count_pairs += dc;
     S.union_pairs += du;
     S.border_pairs += db;
-    S.count_pair_dims += dc * D;
+    S.count_pair_dims += dc * D - ((int64_t)h_skipped - S.count_skipped_dims);
+    S.count_skipped_dims = (int64_t)h_skipped;
     S.union_pair_dims += du * D;
     S.border_pair_dims += db * D;
     S.n_valid += nv;
@@ -1556,6 +1697,8 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
         jd.list_cap = std::max(0, jd.min_pts - 1);
         jd.key_base = key_base;  // every job owns >= 1 key, so the bases increase
         key_base += (unsigned long long)cells;
+        jd.col_base = (long long)std::min(bp.columns, 9e18);  // used only when the table fits its budget
+        bp.columns += grid_columns(pl.g);
         bp.list_stride = std::max(bp.list_stride, jd.list_cap);
         nv += jnv;
     }
@@ -1631,8 +1774,7 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     ndb_status s = check_ctx(ctx);
     if (s != NDB_OK) return s;
     if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return NDB_ERR_INVALID_ARGUMENT;
-    if (flags & ~(NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS | NDB_FLAG_EXACT_COUNT |
-                  NDB_FLAG_TENSOR_FILTER)) return NDB_ERR_INVALID_ARGUMENT;
+    if (flags & ~kAllFlags) return NDB_ERR_INVALID_ARGUMENT;
     ctx->have_state = false;
     ctx->have_labels = false;
     ctx->stats = ndb_stats{};
@@ -1719,6 +1861,7 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
         acc.tensor_items += s1.tensor_items;
         acc.tensor_filter |= s1.tensor_filter;
         acc.count_pair_dims += s1.count_pair_dims;
+        acc.count_skipped_dims += s1.count_skipped_dims;
         acc.union_pair_dims += s1.union_pair_dims;
         acc.border_pair_dims += s1.border_pair_dims;
         acc.ms_grid += s1.ms_grid;
@@ -1734,6 +1877,9 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     }
     acc.solo_jobs = (int32_t)solo.size();
     ctx->stats = acc;
+    // a pipeline reports a device-side failure through its jobs' statuses
+    for (int64_t i = 0; i < n_jobs && first == NDB_OK; ++i)
+        if (jobs[i].status != NDB_OK) first = (ndb_status)jobs[i].status;
     ctx->have_state = false;
     ctx->have_labels = false;
     return first;
@@ -1883,6 +2029,7 @@ extern "C" ndb_status ndb_b200_run_noalloc(const float *coords, int64_t n, int32
     // slice is refused before any cudaFree/cudaMalloc instead of reallocating
     s.ctx.mem_limit = s.ctx.held_bytes();
     s.ctx.list_budget = na_cap(NA_NBR_LIST) - 4;  // lists only where they fit the slice
+    s.ctx.col_budget = 0;  // a column table's size follows the bounding box, not n: cells hashed instead
     s.ctx.own_stream = nullptr;
     s.ctx.stream = static_cast<cudaStream_t>(cuda_stream);
     ndb_status st = ndb_b200_classify(&s.ctx, coords, n, d, eps, min_pts, flags | NDB_FLAG_DEVICE_PTRS, nn_out);

@@ -34,6 +34,20 @@ __device__ __forceinline__ bool in_range(const float (&a)[D], const float (&b)[D
     return len <= e2;
 }
 
+// The same sum in two parts: dimensions [K0, K1) added to len.  Every term is
+// non-negative, and rounding to nearest is monotone, so a partial sum above e2 already
+// decides the pair (out of range) -- the kernels use that to skip the remaining
+// dimensions; continuing the sum gives exactly in_range's length.
+template <int D, int K0, int K1>
+__device__ __forceinline__ float dist_part(const float (&a)[D], const float (&b)[D], float len) {
+#pragma unroll
+    for (int k = K0; k < K1; ++k) {
+        const float t = __fsub_rn(a[k], b[k]);
+        len = __fadd_rn(len, __fmul_rn(t, t));
+    }
+    return len;
+}
+
 template <int D>
 __device__ __forceinline__ void load_point(const float *__restrict__ xs, int64_t idx, float (&x)[D]) {
     constexpr int P = Stride<D>::P;

@@ -58,6 +58,7 @@ struct JobDev {
     int list_cap;                  // neighbour-list entries recorded (min_pts - 1, 0 = none)
     int linked;                    // same-cell-linked grid (cell units)
     unsigned long long key_base;   // first composite cell key of the job
+    long long col_base;            // first entry of the job's columns in the column table
     GridDev g;
     const float *src;              // the job's coordinates (device), gathered into the batch
     int32_t *nn_out;               // caller's outputs (device; may be null)
@@ -297,6 +298,85 @@ __device__ __forceinline__ int hash_find(const K *__restrict__ hkeys, const int3
     return -1;
 }
 
+// ---------------------------------------------------------------------------
+// How cells are found by key.  A column is the run of cells that differ only in
+// gridded dimension 0; sorted by key, a column's cells are contiguous and ordered
+// by x.  When the grid's columns are few enough (their count depends on the
+// bounding box, not on n), a dense table holds each column's [first, end) range
+// of cell indices, so a stencil row is one table load plus a search inside one
+// short column.  Otherwise the open-addressing hash table of the cell keys is
+// probed per x position.
+// ---------------------------------------------------------------------------
+template <typename K>
+struct CellIndex {
+    const int2 *col;      // column table (null: use the hash table)
+    const K *hkeys;
+    const int32_t *hvals;
+    unsigned long long mask;
+};
+
+// Column of every cell: the table entry of its column gets the first cell (the
+// column's first in key order) and the end (one past its last).  The table starts
+// zeroed (empty columns read [0, 0)).
+template <typename K>
+__device__ __forceinline__ long long global_column(const K *__restrict__ cell_key, int64_t c, const GridDev &g_one,
+                                                   const JobDev *__restrict__ jobs,
+                                                   const int32_t *__restrict__ cell_job) {
+    unsigned long long key_base = 0;
+    long long col_base = 0, g0 = g_one.g[0];
+    if (jobs) {
+        const JobDev &J = jobs[cell_job[c]];
+        key_base = J.key_base;
+        col_base = J.col_base;
+        g0 = J.g.g[0];
+    }
+    const unsigned long long local = (unsigned long long)cell_key[c] - key_base;
+    if constexpr (sizeof(K) == 4) return col_base + (long long)((uint32_t)local / (uint32_t)g0);
+    else return col_base + (long long)(local / (unsigned long long)g0);
+}
+
+template <typename K>
+__global__ void col_range_kernel(const K *__restrict__ cell_key, int64_t n_cells, GridDev g_one,
+                                 const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job,
+                                 int2 *__restrict__ col) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    const long long mine = global_column(cell_key, c, g_one, jobs, cell_job);
+    if (c == 0 || global_column(cell_key, c - 1, g_one, jobs, cell_job) != mine) col[mine].x = (int)c;
+    if (c == n_cells - 1 || global_column(cell_key, c + 1, g_one, jobs, cell_job) != mine) col[mine].y = (int)(c + 1);
+}
+
+// First cell of column range cr whose key is >= rowkey + x (cr.y when none); the
+// column's cells have keys rowkey + x' with strictly increasing x'.  A column
+// without gaps places it directly: position first + (x - x_first).
+template <typename K>
+__device__ __forceinline__ int col_lower(const K *__restrict__ cell_key, int2 cr, unsigned long long rowkey,
+                                         long long x) {
+    if (cr.x >= cr.y) return cr.y;
+    const long long xf = (long long)((unsigned long long)__ldg(cell_key + cr.x) - rowkey);
+    if (x <= xf) return cr.x;
+    const long long p = cr.x + (x - xf);  // keys grow by >= 1 per cell: key[p] >= rowkey + x
+    if (p < cr.y && (unsigned long long)__ldg(cell_key + p) == rowkey + (unsigned long long)x) return (int)p;
+    int lo = cr.x + 1, hi = (int)(p < cr.y ? p : cr.y);
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((unsigned long long)__ldg(cell_key + mid) < rowkey + (unsigned long long)x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Cell index of the cell with key rowkey + x in column ncol, or -1.
+template <typename K>
+__device__ __forceinline__ int find_cell(const CellIndex<K> &L, const K *__restrict__ cell_key, long long ncol,
+                                         unsigned long long rowkey, long long x) {
+    const unsigned long long key = rowkey + (unsigned long long)x;
+    if (!L.col) return hash_find(L.hkeys, L.hvals, L.mask, key);
+    const int2 cr = __ldg(L.col + ncol);
+    const int a = col_lower(cell_key, cr, rowkey, x);
+    return a < cr.y && (unsigned long long)__ldg(cell_key + a) == key ? a : -1;
+}
+
 // nbr[c * n_rows + r] = [first, last) cell index of row r around cell c: the cells
 // of a row have consecutive keys, so the existing ones are consecutive in the
 // sorted cell list and the range runs from the smallest to the largest found.
@@ -349,9 +429,8 @@ __device__ __forceinline__ void decode_key(K key, const GridDev &g, long long &x
 template <typename K>
 __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell_key, int64_t n_cells,
                                                       GridDev g_one, const int4 *__restrict__ rows, int n_rows,
-                                                      int group_log2, const K *__restrict__ hkeys,
-                                                      const int32_t *__restrict__ hvals, unsigned long long mask,
-                                                      int2 *__restrict__ nbr, const JobDev *__restrict__ jobs,
+                                                      int group_log2, CellIndex<K> L, int2 *__restrict__ nbr,
+                                                      const JobDev *__restrict__ jobs,
                                                       const int32_t *__restrict__ cell_job) {
     // one lane per (cell, row): 2^group_log2 lanes (>= n_rows) per cell, so
     // a cell's rows are looked up in parallel and its row table is written at once
@@ -363,11 +442,13 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
     const int r = (int)(gid & ((1 << group_log2) - 1));
     if (c >= n_cells || r >= n_rows) return;
     unsigned long long key_base = 0;
+    long long col_base = 0;
     GridDev g = g_one;
     if (jobs) {
         const JobDev &J = jobs[cell_job[c]];
         g = J.g;
         key_base = J.key_base;
+        col_base = J.col_base;
     }
     long long cc[kMaxGridDims];
     decode_key<K>((K)((unsigned long long)cell_key[c] - key_base), g, cc);
@@ -375,12 +456,15 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
     const int off[kMaxGridDims] = {0, row.x, row.y, row.z};
     bool in = true;
     unsigned long long base = key_base;
+    long long ncol = 0, cstride = 1;  // the row's column: cells differing only in dimension 0
 #pragma unroll
     for (int a = 1; a < kMaxGridDims; ++a) {
         if (a < g.k) {
             const long long v = cc[a] + off[a];
             in = in && v >= 0 && v < g.g[a];
             base += (unsigned long long)(v < 0 ? 0 : v) * g.stride[a];
+            ncol += (v < 0 ? 0 : v) * cstride;
+            cstride *= g.g[a];
         }
     }
     int2 res = make_int2(0, 0);
@@ -388,10 +472,17 @@ __global__ void __launch_bounds__(kBlock) rows_kernel(const K *__restrict__ cell
         const long long x0 = cc[0] - row.w < 0 ? 0 : cc[0] - row.w;
         const long long x1 = cc[0] + row.w > g.g[0] - 1 ? g.g[0] - 1 : cc[0] + row.w;
         // the row's existing cells are consecutive in the sorted cell list: find the
-        // first one by hashing (usually the first probe, at x0), then count the keys
-        // that follow it within the row (independent loads, at most 2 row.w of them)
+        // first one (a column-table search, or hashing from x0 on), then count the
+        // keys that follow it within the row (independent loads, at most 2 row.w)
         int ca = -1;
-        for (long long xx = x0; xx <= x1 && ca < 0; ++xx) ca = hash_find(hkeys, hvals, mask, base + (unsigned long long)xx);
+        if (L.col) {
+            const int2 cr = __ldg(L.col + col_base + ncol);
+            const int a = col_lower(cell_key, cr, base, x0);
+            if (a < cr.y && (unsigned long long)__ldg(cell_key + a) <= base + (unsigned long long)x1) ca = a;
+        } else {
+            for (long long xx = x0; xx <= x1 && ca < 0; ++xx)
+                ca = hash_find(L.hkeys, L.hvals, L.mask, base + (unsigned long long)xx);
+        }
         if (ca >= 0) {
             // keys are sorted and unique: the row's cells after ca are a prefix of the
             // next keys; four independent loads cover rows of up to 5 cells
@@ -541,7 +632,8 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts,
     int dense_skip, int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap,
     int list_stride, unsigned long long *__restrict__ pair_counter, const JobDev *__restrict__ jobs,
-    const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr) {
+    const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev,
+    unsigned long long *__restrict__ skipped_dims) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kCountWarps][kTile * P];
     __shared__ RowTable s_rows[kCountWarps];
@@ -580,7 +672,8 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     __syncwarp();
     // running counts in registers: lane k holds the count of the item's point k
     int mycnt = 0;
-    unsigned long long pairs = 0;
+    unsigned long long pairs = 0, skipped = 0;  // pairs tested; pairs whose second half was skipped
+    int halves = 0;
     // points still counting (EARLY: below min_pts), and points whose neighbour list
     // is still filling (count below list_cap): both warp-uniform, updated per chunk
     unsigned act = __ballot_sync(kFull, lane < cnt);
@@ -607,8 +700,28 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
             load_point_smem<D>(si + k * P, xi);
             bool hit[CH];
             unsigned m[CH];
+            if constexpr (D >= 8) {
+                // the first half of the sum; when no lane's pair can still be in range
+                // the warp skips the second half (exact: the partial sums only grow)
+                constexpr int H = D / 2;
+                float len[CH];
 #pragma unroll
-            for (int c = 0; c < CH; ++c) hit[c] = in_range<D>(xi, xj[c], e2);
+                for (int c = 0; c < CH; ++c) len[c] = dist_part<D, 0, H>(xi, xj[c], 0.0f);
+                bool open = false;
+#pragma unroll
+                for (int c = 0; c < CH; ++c) open = open || len[c] <= e2;
+                if (__any_sync(kFull, open)) {
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) hit[c] = dist_part<D, H, D>(xi, xj[c], len[c]) <= e2;
+                } else {
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) hit[c] = false;
+                    ++halves;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < CH; ++c) hit[c] = in_range<D>(xi, xj[c], e2);
+            }
 #pragma unroll
             for (int c = 0; c < CH; ++c) m[c] = __ballot_sync(kFull, hit[c]);
             // the first list_cap neighbours of each point; complete for every point
@@ -632,6 +745,8 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
             ++active;
         }
         pairs += (unsigned long long)active * (unsigned long long)min(kWarp * CH, total - tb);
+        skipped += (unsigned long long)halves * (unsigned long long)min(kWarp * CH, total - tb);
+        halves = 0;
         if (lst) lst &= __ballot_sync(kFull, mycnt < list_cap);
         if (EARLY) {
             act = __ballot_sync(kFull, lane < cnt && mycnt < min_pts);
@@ -650,6 +765,7 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
         }
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
+    if (lane == 0 && skipped) atomicAdd(skipped_dims, skipped * (unsigned long long)(D - D / 2));
 }
 
 // Core flags: per sorted point (u8), and a bitmap in input order (one bit per
@@ -808,8 +924,7 @@ __device__ __forceinline__ void load_first_cores(const float *__restrict__ xs, c
 template <int D, typename K>
 __global__ void __launch_bounds__(kBlock) union_near_kernel(
     int64_t n_cells, GridDev g_one, const K *__restrict__ cell_key, const int32_t *__restrict__ cell_start,
-    const K *__restrict__ hkeys, const int32_t *__restrict__ hvals, unsigned long long mask,
-    const float *__restrict__ xs, float e2, const uint8_t *__restrict__ core_sorted,
+    CellIndex<K> L, const float *__restrict__ xs, float e2, const uint8_t *__restrict__ core_sorted,
     const uint8_t *__restrict__ cell_has_core, int32_t *parent, unsigned long long *__restrict__ pair_counter,
     int *err, const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -819,18 +934,24 @@ __global__ void __launch_bounds__(kBlock) union_near_kernel(
         const unsigned long long key = (unsigned long long)cell_key[A];
         GridDev g = g_one;
         unsigned long long key_base = 0;
+        long long col_base = 0;
         if (jobs) {
             const JobDev &J = jobs[cell_job[A]];
             g = J.g;
             e2 = J.e2;
             key_base = J.key_base;
+            col_base = J.col_base;
         }
         long long cc[kMaxGridDims];
         decode_key<K>((K)(key - key_base), g, cc);
+        // the cell's column, and the keys of x = 0 in the columns one step up in y and z
+        const long long col = col_base + cc[1] + (g.k >= 3 ? cc[2] * g.g[1] : 0);
+        const unsigned long long row0 = key - (unsigned long long)cc[0];
         int nb[3] = {-1, -1, -1};
         if (cc[0] + 1 < g.g[0] && A + 1 < n_cells && (unsigned long long)cell_key[A + 1] == key + 1ull) nb[0] = A + 1;
-        if (g.k >= 2 && cc[1] + 1 < g.g[1]) nb[1] = hash_find(hkeys, hvals, mask, key + g.stride[1]);
-        if (g.k >= 3 && cc[2] + 1 < g.g[2]) nb[2] = hash_find(hkeys, hvals, mask, key + g.stride[2]);
+        if (g.k >= 2 && cc[1] + 1 < g.g[1]) nb[1] = find_cell(L, cell_key, col + 1, row0 + g.stride[1], cc[0]);
+        if (g.k >= 3 && cc[2] + 1 < g.g[2])
+            nb[2] = find_cell(L, cell_key, col + g.g[1], row0 + g.stride[2], cc[0]);
         bool any = false;
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
@@ -1493,6 +1614,35 @@ __global__ void output_ci_kernel(const int32_t *__restrict__ ci_sorted, int64_t 
         if (noise) atomicAdd(counters + 1, (unsigned long long)noise);
         if (roots) atomicAdd(counters + 0, (unsigned long long)roots);
     }
+}
+
+// ndb_b200_assign_border: the caller's id of every core (input order) into the
+// sorted ids and the cells' ids, which the border kernels read; non-cores start
+// over at NO_CLUSTER.  The cores of one cell are one component, so they carry one id.
+__global__ void set_core_ids_kernel(int64_t nv, const uint8_t *__restrict__ core_sorted,
+                                    const int32_t *__restrict__ perm, const int32_t *__restrict__ ids,
+                                    const int32_t *__restrict__ pcell, int cell_units, int32_t *__restrict__ ci_sorted,
+                                    int32_t *__restrict__ cell_cid) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nv) return;
+    if (core_sorted[s]) {
+        const int32_t v = ids[perm[s]];
+        ci_sorted[s] = v;
+        if (cell_units) cell_cid[pcell[s]] = v;
+    } else {
+        ci_sorted[s] = kNoCluster;
+    }
+}
+
+// Ids in input order after ndb_b200_assign_border: the border pass's ids, and the
+// caller's for cores outside the grid.
+__global__ void output_ids_kernel(const int32_t *__restrict__ ci_sorted, int64_t nv, int64_t n,
+                                  const int32_t *__restrict__ perm, const uint32_t *__restrict__ core_bits,
+                                  const int32_t *__restrict__ ids, int32_t *__restrict__ out) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int32_t o = perm[s];
+    out[o] = s < nv ? ci_sorted[s] : (is_core_o(core_bits, o) ? ids[o] : kNoCluster);
 }
 
 // v_cluster_label in canonical form, on request: labels[rank(o)] = id of core o.

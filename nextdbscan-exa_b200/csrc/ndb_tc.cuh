@@ -185,14 +185,68 @@ __device__ __forceinline__ float centre_split(const float (&x)[D], const float (
 // Neighbour lists: the first list_cap hits of each column (complete for every
 // point that stays below min_pts), slots reserved by shared-memory atomics.
 // ---------------------------------------------------------------------------
+// Audit of the filter (AUDIT, a diagnostic run, never the timed one): every pair the
+// filter classifies is also measured against its FP64 distance and the reference's
+// FP32 predicate.  audit[0] = largest |D~ - d64| (bits of a non-negative double),
+// audit[1] = largest |D~ - d64| / (kappa (n_i + n_j)), the error over the bound the
+// guard band is built from, audit[2] = pairs audited, audit[3] = pairs decided
+// outside the band (hit or miss without a recheck) whose decision differs from the
+// reference's predicate.  D~ = v + |b_j|^2 is the filter's squared distance.
 template <int D>
+__device__ __forceinline__ void audit_tile(const float *s_x, const float *s_ni, const uint32_t (&g)[32], unsigned act,
+                                           unsigned hit, unsigned band, int j, float nj, const float *__restrict__ xs,
+                                           float e2, float kap, unsigned long long *audit) {
+    constexpr int P = Stride<D>::P;
+    double mx = 0.0, mr = 0.0;
+    unsigned cnt = 0, mis = 0;
+    if (j >= 0) {
+        float xj[D];
+        load_point<D>(xs, j, xj);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            if (!((act >> c) & 1u)) continue;
+            float xi[D];
+            load_point_smem<D>(s_x + c * P, xi);
+            double d64 = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const double t = (double)xi[k] - (double)xj[k];
+                d64 = fma(t, t, d64);
+            }
+            const float v = __fmaf_rn(-2.0f, __uint_as_float(g[c]), s_ni[c]);
+            const double err = fabs(((double)v + (double)nj) - d64);
+            const double bound = (double)kap * ((double)s_ni[c] + (double)nj);
+            mx = fmax(mx, err);
+            if (bound > 0.0) mr = fmax(mr, err / bound);
+            ++cnt;
+            const bool exact = in_range<D>(xi, xj, e2);
+            if (!((band >> c) & 1u) && (((hit >> c) & 1u) != 0) != exact) ++mis;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(kFull, mx, o));
+        mr = fmax(mr, __shfl_xor_sync(kFull, mr, o));
+        cnt += __shfl_xor_sync(kFull, cnt, o);
+        mis += __shfl_xor_sync(kFull, mis, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (mx > 0.0) atomicMax(audit + 0, (unsigned long long)__double_as_longlong(mx));
+        if (mr > 0.0) atomicMax(audit + 1, (unsigned long long)__double_as_longlong(mr));
+        if (cnt) atomicAdd(audit + 2, (unsigned long long)cnt);
+        if (mis) atomicAdd(audit + 3, (unsigned long long)mis);
+    }
+}
+
+template <int D, bool AUDIT = false>
 __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts, int early,
     int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
     unsigned long long *__restrict__ pair_counter, unsigned long long *__restrict__ band_counter,
     unsigned int *__restrict__ work, int *__restrict__ err, const JobDev *__restrict__ jobs,
-    const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr) {
+    const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr,
+    unsigned long long *__restrict__ audit = nullptr) {
     constexpr int KP = KPad<D>::v, P = Stride<D>::P, KC = KP / 4;
     __shared__ __align__(1024) uint32_t s_a[2][2][KC * kM * 4];  // [buffer][hi, lo] candidate tiles
     __shared__ __align__(128) uint32_t s_b[2][KC * kN * 4];      // [hi, lo] the item's points
@@ -287,7 +341,7 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
                 load_point<D>(xs, jrow, x);
             }
         };
-        auto stage = [&](int buf, int jrow, const float (&x)[D], float &tlo, float &thi) {
+        auto stage = [&](int buf, int jrow, const float (&x)[D], float &tlo, float &thi, float &nj) {
             uint32_t hi[KP], lo[KP];
             float n = 0.0f;
             if (jrow >= 0) {
@@ -300,6 +354,7 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
             store_row<KP>(s_a[buf][1], kM, tid, lo);
             s_j[buf][tid] = jrow;
             const float slack = __fadd_rn(__fmul_rn(kap, __fadd_rn(nmax, n)), __fmul_rn(kSigma, e2j));
+            nj = n;
             tlo = jrow >= 0 ? __fsub_rn(__fsub_rn(e2lo, n), slack) : -INFINITY;
             thi = jrow >= 0 ? __fadd_rn(__fsub_rn(e2hi, n), slack) : -INFINITY;
         };
@@ -322,9 +377,10 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
 
         int j_cur = -1, j_nxt = -1;
         float tlo_cur = -INFINITY, thi_cur = -INFINITY, tlo_nxt = -INFINITY, thi_nxt = -INFINITY;
+        float nj_cur = 0.0f, nj_nxt = 0.0f;
         float x_nxt[D];
         fetch(0, j_cur, x_nxt);
-        stage(0, j_cur, x_nxt, tlo_cur, thi_cur);
+        stage(0, j_cur, x_nxt, tlo_cur, thi_cur, nj_cur);
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
@@ -351,6 +407,7 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
                     }
                 }
                 bb &= ~hb;
+                if constexpr (AUDIT) audit_tile<D>(s_x, s_ni, g, act, hb, bb, j_cur, nj_cur, xs, e2j, kap, audit);
                 if (__any_sync(kFull, bb != 0)) {
                     if (bb) {
                         float xj[D];
@@ -380,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
                 s_abort = 1;
                 atomicExch(err, 2);
             }
-            if (t < n_tiles) stage(t & 1, j_nxt, x_nxt, tlo_nxt, thi_nxt);
+            if (t < n_tiles) stage(t & 1, j_nxt, x_nxt, tlo_nxt, thi_nxt, nj_nxt);
             fence_async_smem();
             tc_before_sync();
             __syncthreads();
@@ -394,6 +451,7 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
                 pending |= 1u << (t & 1);
                 j_cur = j_nxt;
                 tlo_cur = tlo_nxt;
+                nj_cur = nj_nxt;
                 thi_cur = thi_nxt;
             }
         }

@@ -20,6 +20,7 @@ FLAG_FULL_COUNT = 0x2
 FLAG_DEVICE_PTRS = 0x4
 FLAG_EXACT_COUNT = 0x8
 FLAG_TENSOR_FILTER = 0x10
+FLAG_FILTER_AUDIT = 0x20
 
 STATUS = {
     0: "NDB_OK",
@@ -45,6 +46,7 @@ EXPORTED = (
     "ndb_b200_run",
     "ndb_b200_run_batched",
     "ndb_b200_cluster_label",
+    "ndb_b200_assign_border",
     "ndb_b200_get_stats",
     "ndb_b200_set_memory_limit",
     "ndb_b200_device_bytes",
@@ -110,6 +112,11 @@ class NdbStats(ctypes.Structure):
         ("tensor_filter", ctypes.c_int32),
         ("band_pairs", ctypes.c_int64),
         ("tensor_items", ctypes.c_int64),
+        ("filter_max_abs_err", ctypes.c_double),
+        ("filter_max_err_over_bound", ctypes.c_double),
+        ("filter_audited_pairs", ctypes.c_int64),
+        ("filter_misclassified_pairs", ctypes.c_int64),
+        ("count_skipped_dims", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -155,6 +162,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_run_batched.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbJob), ctypes.c_int64,
                                              ctypes.c_uint32]
         lib.ndb_b200_cluster_label.argtypes = [ctypes.c_void_p, i32p, ctypes.c_int64]
+        lib.ndb_b200_assign_border.argtypes = [ctypes.c_void_p, i32p, i32p]
         lib.ndb_b200_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbStats)]
         lib.ndb_b200_set_memory_limit.argtypes = [ctypes.c_void_p, ctypes.c_int64]
         lib.ndb_b200_device_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
@@ -168,6 +176,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_version.restype = ctypes.c_char_p
         for name in ("ndb_b200_create", "ndb_b200_destroy", "ndb_b200_set_stream", "ndb_b200_classify",
                      "ndb_b200_assign_labels", "ndb_b200_run", "ndb_b200_run_batched", "ndb_b200_cluster_label",
+                     "ndb_b200_assign_border",
                      "ndb_b200_get_stats", "ndb_b200_set_memory_limit", "ndb_b200_device_bytes",
                      "ndb_b200_set_tuning", "ndb_b200_get_tuning", "ndb_b200_set_debug_limits"):
             getattr(lib, name).restype = ctypes.c_int

@@ -149,11 +149,17 @@ def _eps_4nn(rng: np.random.Generator, pts: np.ndarray) -> float:
     return float(np.percentile(dist[:, 4], 90))
 
 
+def _job_shape(rng: np.random.Generator, n_min: int, n_max: int, dims) -> tuple[int, int]:
+    """The first two draws of a batch job: its n (log-uniform) and its d."""
+    n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+    d = int(dims[rng.integers(0, len(dims))])
+    return n, d
+
+
 def _one_job(args) -> BatchJob:
     seq, n_min, n_max, dims = args
     rng = np.random.Generator(np.random.PCG64(seq))
-    n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
-    d = int(dims[rng.integers(0, len(dims))])
+    n, d = _job_shape(rng, n_min, n_max, dims)
     k = int(rng.integers(5, 51))
     n_noise = int(round(n * 0.05))
     centers = rng.uniform(0.0, 100.0, (k, d))
@@ -182,6 +188,14 @@ def config4(n_jobs: int = 4096, seed: int = 4, n_min: int = 1_000, n_max: int = 
 
     with mp.get_context("spawn").Pool(workers) as pool:  # spawn: callers may already hold a CUDA context
         return pool.map(_one_job, args, chunksize=max(1, n_jobs // (8 * workers)))
+
+
+def config4_shapes(n_jobs: int = 4096, seed: int = 4, n_min: int = 1_000, n_max: int = 200_000,
+                   dims: tuple = (2, 3, 8, 16)) -> list[tuple[int, int]]:
+    """(n, d) of every job of config4 with the same arguments, without drawing the
+    points (for sizing and extrapolation)."""
+    return [_job_shape(np.random.Generator(np.random.PCG64(s)), n_min, n_max, tuple(dims))
+            for s in np.random.SeedSequence(seed).spawn(n_jobs)]
 
 
 CONFIGS = {1: config1, 2: config2, 3: config3, 5: config5}

@@ -7,6 +7,7 @@ thing measured on the GPU or shipped.
   reference(...)  literal restatement of the reference's phases (ndb_oracle.c)
   grid(...)       exact grid restatement of the same outputs (ndb_oracle.c)
   cells(...)      the same outputs organised for 10^7..10^8 points (ndb_oracle.c)
+  border_ids(...) the border rule with given core ids (ndb_oracle.c)
   run_ref(...)    the reference's own OpenMP implementation, built from its
                   sources into _ref/ndb_ref_harness by oracle/Makefile
 """
@@ -65,6 +66,9 @@ def _load() -> ctypes.CDLL:
         lib.ndb_oracle_cells.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
                                          ctypes.c_int32, vp, vp, vp]
         lib.ndb_oracle_cells.restype = ctypes.c_int
+        lib.ndb_oracle_border_ids.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
+                                              vp, vp, vp]
+        lib.ndb_oracle_border_ids.restype = ctypes.c_int
         lib.ndb_oracle_threads.restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -123,6 +127,21 @@ def cells(coords, eps: float, min_pts: int, early: bool = False):
         raise RuntimeError(f"ndb_oracle_cells failed: {rc}")
     return nn, ci, dict(clusters=int(meta[0]), noise=int(meta[1]), cores=int(meta[2]), n=int(meta[3]),
                         clique_cells=bool(meta[4]))
+
+
+def border_ids(coords, eps: float, min_pts: int, nn, ids):
+    """The border rule with given core ids (brute force): cores keep ids[i], every
+    other point takes the minimum id over the cores in range.  Returns the ids."""
+    a = _pts(coords)
+    n, d = a.shape
+    nn = np.ascontiguousarray(np.asarray(nn, dtype=np.int32))
+    ids = np.ascontiguousarray(np.asarray(ids, dtype=np.int32))
+    out = np.zeros(n, np.int32)
+    rc = _load().ndb_oracle_border_ids(a.ctypes.data, n, d, ctypes.c_float(eps), int(min_pts), nn.ctypes.data,
+                                       ids.ctypes.data, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ndb_oracle_border_ids failed: {rc}")
+    return out
 
 
 def threads() -> int:

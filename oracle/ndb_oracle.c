@@ -942,6 +942,38 @@ int ndb_oracle_cells(const float *coord, int64_t n, int32_t d, float e, int32_t 
     return 0;
 }
 
+/*
+ * ndb_oracle_border_ids -- the border rule (data_process.cpp:204-209) with given
+ * core ids: every non-core point takes the minimum of ids[j] over the core points j
+ * in range (the reference's FP32 predicate), NO_CLUSTER when there is none; a core
+ * keeps ids[i].  Cores are nn[i] >= m.  Brute force over all pairs (small inputs:
+ * the checker of the sharded form's border pass).  Returns 0, or -2 when e*e is not
+ * finite.
+ */
+int ndb_oracle_border_ids(const float *coord, int64_t n, int32_t d, float e, int32_t m, const int32_t *nn,
+                          const int32_t *ids, int32_t *out) {
+    const float e2 = e * e;
+    if (!isfinite(e2)) return -2;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        if (nn[i] >= m) {
+            out[i] = ids[i];
+            continue;
+        }
+        int32_t best = NDB_ORACLE_NO_CLUSTER;
+        const float *p1 = coord + i * d;
+        if (point_valid(p1, d)) {
+            for (int64_t j = 0; j < n; ++j) {
+                if (nn[j] < m || ids[j] >= best) continue;
+                if (!point_valid(coord + j * d, d)) continue;
+                if (in_range(p1, coord + j * d, d, e2)) best = ids[j];
+            }
+        }
+        out[i] = best;
+    }
+    return 0;
+}
+
 /* Number of OpenMP threads the grid oracle uses (1 without OpenMP). */
 int ndb_oracle_threads(void) {
 #ifdef _OPENMP

@@ -151,3 +151,23 @@ def test_tuning_and_autotuner(ctx, pkg):
     finally:
         ctx.reset_tuning()
     assert ctx.tuning() == {"tc_min_dim": 0, "tc_min_item": 0}
+
+
+@pytest.mark.parametrize("full", [True, False])
+def test_filter_audit_every_pair_within_its_bound(ctx, pkg, full):
+    """NDB_FLAG_FILTER_AUDIT: every pair the filter classified is measured against
+    its FP64 distance and the exact FP32 predicate.  None is decided wrongly outside
+    the guard band, the error stays inside the bound the band is built from, and the
+    audited run gives the unaudited run's outputs."""
+    w = pkg.synthetic.config3(n=60_000)
+    nn, ci, res = ctx.run(w.coords, w.eps, w.min_pts, full_count=full, tensor_filter=True)
+    nn_a, ci_a, res_a = ctx.run(w.coords, w.eps, w.min_pts, full_count=full, tensor_filter=True, audit=True)
+    s = ctx.stats()
+    assert s["tensor_filter"] == 1
+    assert s["filter_audited_pairs"] > 0
+    assert s["filter_misclassified_pairs"] == 0
+    assert 0.0 < s["filter_max_abs_err"] and s["filter_max_err_over_bound"] <= 1.0
+    np.testing.assert_array_equal(ci_a, ci)
+    if full:
+        np.testing.assert_array_equal(nn_a, nn)
+    assert res_a == res
