@@ -58,7 +58,8 @@ typedef enum ndb_status {
     NDB_ERR_NO_DEVICE = 7,        /* no CUDA device / bad device ordinal */
     NDB_ERR_DEVICE_LIMIT = 8,     /* a device-side loop hit its iteration bound */
     NDB_ERR_NO_STATE = 9,         /* ndb_b200_assign_labels before ndb_b200_classify */
-    NDB_ERR_BAD_JOB = 10          /* a batched job descriptor is invalid */
+    NDB_ERR_BAD_JOB = 10,         /* a batched job descriptor is invalid */
+    NDB_ERR_IO = 11               /* ndb_b200_load_bin: the file is missing, short, or has a bad header */
 } ndb_status;
 
 /* Largest n per job: indices are int32, as in the reference (data_process.h:47-59). */
@@ -160,6 +161,24 @@ ndb_status ndb_b200_assign_labels(ndb_ctx *ctx, int32_t *cluster_index_out, ndb_
 ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps,
                         int32_t min_pts, uint32_t flags, int32_t *nn_out,
                         int32_t *cluster_index_out, ndb_result *result);
+
+/* The reference's binary input file (magma_input.h:113-125: int32 n, int32 d, then
+ * n*d float32 row-major) read straight into the context's device memory: the file
+ * is read in chunks into two pinned staging buffers, each chunk's copy to the device
+ * runs while the next chunk is read, and the bounding box of the grid is reduced
+ * chunk by chunk as the chunks land.  Replaces magma_input::read_input for .bin
+ * files (magma_input.h:144-167) and the host-to-device copy of the data_process
+ * constructor (data_process.h:62).  n and d of the file are returned; the job stays
+ * loaded until the next run or load on the context that is not
+ * ndb_b200_run_loaded.  A missing or short file, or a bad header, is NDB_ERR_IO
+ * (d outside 1..NDB_MAX_DIM is NDB_ERR_UNSUPPORTED_DIM). */
+ndb_status ndb_b200_load_bin(ndb_ctx *ctx, const char *path, int64_t *n, int32_t *d);
+
+/* ndb_b200_run on the job ndb_b200_load_bin loaded (any number of times, with any
+ * eps, min_pts and flags).  Outputs are host pointers, or device pointers with
+ * NDB_FLAG_DEVICE_PTRS; NDB_ERR_NO_STATE when nothing is loaded. */
+ndb_status ndb_b200_run_loaded(ndb_ctx *ctx, float eps, int32_t min_pts, uint32_t flags, int32_t *nn_out,
+                               int32_t *cluster_index_out, ndb_result *result);
 
 /* One job of a batched run: an independent DBSCAN problem with its own
  * coordinates, dimensionality, eps and min_pts (the arguments of one

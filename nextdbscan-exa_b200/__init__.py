@@ -67,6 +67,7 @@ class Context:
         self._h = h
         self.device = device
         self.n = 0
+        self._loaded = (0, 0)
 
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
@@ -128,6 +129,31 @@ class Context:
         st = self._lib.ndb_b200_run(self._h, pts.ctypes.data, n, d, ctypes.c_float(eps), int(min_pts), flags,
                                     nn.ctypes.data, ci.ctypes.data, ctypes.byref(res))
         lib.check(st, "ndb_b200_run", self._h)
+        self.n = n
+        return nn, ci, Result(res.clusters, res.noise, res.core_count, res.n)
+
+    # -- the reference's .bin file straight to the device (pinned, chunked, overlapped) --
+    def load_bin(self, path: str) -> tuple[int, int]:
+        """Loads a .bin file (int32 n, int32 d, n*d float32) into the context's device
+        memory through pinned chunks; returns (n, d).  See ndb_b200_load_bin."""
+        n = ctypes.c_int64()
+        d = ctypes.c_int32()
+        st = self._lib.ndb_b200_load_bin(self._h, str(path).encode(), ctypes.byref(n), ctypes.byref(d))
+        lib.check(st, "ndb_b200_load_bin", self._h)
+        self.n, self._loaded = n.value, (n.value, d.value)
+        return n.value, d.value
+
+    def run_loaded(self, eps: float, min_pts: int, *, full_count: bool = False, approximate: bool = False,
+                   exact_count: bool = False, tensor_filter: bool = False) -> tuple[np.ndarray, np.ndarray, Result]:
+        """ndb_b200_run on the loaded job, outputs in host memory."""
+        n = self._loaded[0]
+        nn = np.empty(n, dtype=np.int32)
+        ci = np.empty(n, dtype=np.int32)
+        res = lib.NdbResult()
+        st = self._lib.ndb_b200_run_loaded(self._h, ctypes.c_float(eps), int(min_pts),
+                                           _flags(full_count, approximate, exact_count, tensor_filter),
+                                           nn.ctypes.data, ci.ctypes.data, ctypes.byref(res))
+        lib.check(st, "ndb_b200_run_loaded", self._h)
         self.n = n
         return nn, ci, Result(res.clusters, res.noise, res.core_count, res.n)
 

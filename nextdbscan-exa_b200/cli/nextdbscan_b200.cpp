@@ -1,6 +1,7 @@
 // nextdbscan_b200.cpp -- command-line front end with the reference's flags
-// (main.cpp:57-129), running the B200 hot path through the C++ drop-in
-// (ndb_b200_data_process.h) and the C ABI.
+// (main.cpp:57-129), running the B200 hot path through the C ABI (.bin input:
+// ndb_b200_load_bin, file to device through pinned chunks) or the C++ drop-in
+// (ndb_b200_data_process.h; .csv input).
 //
 //   nextdbscan-b200 -m minPts -e eps [-t threads] [-a 0|1] [-o labels.txt] input.bin|input.csv
 //
@@ -45,6 +46,20 @@ void usage() {
     std::cout << ".bin: int32 n, int32 d, then n*d float32 values" << std::endl;
 }
 
+bool has_suffix(const std::string &s, const char *suf) {
+    const std::string x(suf);
+    return s.size() >= x.size() && s.compare(s.size() - x.size(), x.size(), x) == 0;
+}
+
+// The library's status as the reference treats hard errors: print and exit.
+void check(ndb_status s, const char *where, ndb_ctx *ctx) {
+    if (s == NDB_OK) return;
+    std::cerr << "nextdbscan-b200: " << where << ": " << ndb_b200_strerror(s);
+    if (ctx && *ndb_b200_last_cuda_error(ctx)) std::cerr << " (" << ndb_b200_last_cuda_error(ctx) << ")";
+    std::cerr << std::endl;
+    std::exit(EXIT_FAILURE);
+}
+
 long long ms_since(std::chrono::steady_clock::time_point t) {
     return std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t).count();
 }
@@ -78,26 +93,58 @@ int main(int argc, char **argv) {
               << " a: " << a << std::endl;
 
     auto t0 = std::chrono::steady_clock::now();
-    std::vector<float> v_coord;
-    int n_total = -1, n_dim = -1;
-    if (!ndb_input::read_input(input_file, v_coord, n_total, n_dim)) return EXIT_FAILURE;
-    std::cout << "Read Input Data: " << ms_since(t0) << " milliseconds" << std::endl;
-    std::cout << "Read " << n_total << " aggregated points with " << n_dim << " dimensions. " << std::endl;
-
-    auto t1 = std::chrono::steady_clock::now();
-    data_process dp(v_coord, m, e, n_dim, n_total, a == 1);
-    dp.full_count = f == 1;
-    one_rank mpi;
-    auto tc = std::chrono::steady_clock::now();
-    dp.select_and_process(mpi);
-    std::cout << "Classify Points: " << ms_since(tc) << " milliseconds" << std::endl;
-    auto tl = std::chrono::steady_clock::now();
-    dp.select_cores_and_process(mpi);
-    std::cout << "Assign Labels: " << ms_since(tl) << " milliseconds" << std::endl;
     int cores = 0, noise = 0, clusters = 0, n = 0;
-    dp.get_result_meta(cores, noise, clusters, n, mpi);
-    std::cout << "Total Execution Time: " << ms_since(t0) << " milliseconds" << std::endl;
-    std::cout << "Total Execution Time (without I/O): " << ms_since(t1) << " milliseconds" << std::endl;
+    std::vector<int> cluster_index;
+    const uint32_t flags = (f == 1 ? NDB_FLAG_FULL_COUNT : 0u) | (a == 1 ? NDB_FLAG_APPROXIMATE : 0u);
+    if (has_suffix(input_file, ".bin")) {
+        // the binary input goes straight from the file to the device: pinned chunks,
+        // each copied while the next is read (ndb_b200_load_bin)
+        ndb_ctx *ctx = nullptr;
+        check(ndb_b200_create(&ctx, 0), "ndb_b200_create", nullptr);
+        int64_t n_total = 0;
+        int32_t n_dim = 0;
+        check(ndb_b200_load_bin(ctx, input_file.c_str(), &n_total, &n_dim), "ndb_b200_load_bin", ctx);
+        std::cout << "Read Input Data: " << ms_since(t0) << " milliseconds" << std::endl;
+        std::cout << "Read " << n_total << " aggregated points with " << n_dim << " dimensions. " << std::endl;
+        auto t1 = std::chrono::steady_clock::now();
+        std::vector<int> nn((size_t)n_total);
+        cluster_index.resize((size_t)n_total);
+        ndb_result r{};
+        check(ndb_b200_run_loaded(ctx, e, m, flags, nn.data(), cluster_index.data(), &r), "ndb_b200_run_loaded", ctx);
+        ndb_stats st{};
+        ndb_b200_get_stats(ctx, &st);
+        // phase times of the reference's printout (nextdbscan.cpp:48-57), from the device events
+        std::cout << "Classify Points: " << (long long)(st.ms_grid + st.ms_count) << " milliseconds" << std::endl;
+        std::cout << "Assign Labels: " << (long long)(st.ms_union + st.ms_border) << " milliseconds" << std::endl;
+        cores = r.core_count;
+        noise = r.noise;
+        clusters = r.clusters;
+        n = r.n;
+        ndb_b200_destroy(ctx);
+        std::cout << "Total Execution Time: " << ms_since(t0) << " milliseconds" << std::endl;
+        std::cout << "Total Execution Time (without I/O): " << ms_since(t1) << " milliseconds" << std::endl;
+    } else {
+        std::vector<float> v_coord;
+        int n_total = -1, n_dim = -1;
+        if (!ndb_input::read_input(input_file, v_coord, n_total, n_dim)) return EXIT_FAILURE;
+        std::cout << "Read Input Data: " << ms_since(t0) << " milliseconds" << std::endl;
+        std::cout << "Read " << n_total << " aggregated points with " << n_dim << " dimensions. " << std::endl;
+
+        auto t1 = std::chrono::steady_clock::now();
+        data_process dp(v_coord, m, e, n_dim, n_total, a == 1);
+        dp.full_count = f == 1;
+        one_rank mpi;
+        auto tc = std::chrono::steady_clock::now();
+        dp.select_and_process(mpi);
+        std::cout << "Classify Points: " << ms_since(tc) << " milliseconds" << std::endl;
+        auto tl = std::chrono::steady_clock::now();
+        dp.select_cores_and_process(mpi);
+        std::cout << "Assign Labels: " << ms_since(tl) << " milliseconds" << std::endl;
+        dp.get_result_meta(cores, noise, clusters, n, mpi);
+        cluster_index = std::move(dp.v_coord_cluster_index);
+        std::cout << "Total Execution Time: " << ms_since(t0) << " milliseconds" << std::endl;
+        std::cout << "Total Execution Time (without I/O): " << ms_since(t1) << " milliseconds" << std::endl;
+    }
 
     std::cout << std::endl;
     if (a == 0) std::cout << "Estimated Clusters: " << clusters << std::endl;
@@ -113,9 +160,9 @@ int main(int argc, char **argv) {
             return EXIT_FAILURE;
         }
         std::string buf;
-        buf.reserve(dp.v_coord_cluster_index.size() * 8);
+        buf.reserve(cluster_index.size() * 8);
         char tmp[16];
-        for (int c : dp.v_coord_cluster_index) {
+        for (int c : cluster_index) {
             int len = std::snprintf(tmp, sizeof(tmp), "%d\n", c);
             buf.append(tmp, (size_t)len);
         }

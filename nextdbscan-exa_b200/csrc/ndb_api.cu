@@ -57,6 +57,19 @@ struct ndb_ctx {
     DevBuf items_split;
     // caller's core ids of ndb_b200_assign_border (host inputs)
     DevBuf ids_in;
+    // batched runs on host buffers: every job's coordinates and outputs on the device
+    DevBuf batch_in, batch_nn, batch_ci;
+    cudaEvent_t ev_grp[NDB_MAX_DIM + 1] = {};  // a group's inputs are on the device
+    cudaEvent_t ev_out = nullptr;              // a group's outputs are ready
+    // ndb_b200_load_bin: two pinned staging chunks, the loaded job (its coordinates in
+    // `coords`) and its bounding box, reduced chunk by chunk while it arrived
+    void *pin[2] = {nullptr, nullptr};
+    size_t pin_bytes = 0;
+    cudaEvent_t ev_pin[2] = {nullptr, nullptr};
+    DevBuf load_box;
+    bool loaded = false;
+    int64_t loaded_n = 0;
+    int loaded_d = 0;
     // largest device footprint the context may hold (bytes); 0 = no cap
     size_t mem_limit = 0;
     // count-kernel thresholds set by ndb_b200_set_tuning (0: the library's defaults)
@@ -72,7 +85,8 @@ struct ndb_ctx {
                           &cell_key,    &nbr,         &item_cnt,    &items,       &cell_has_core, &cell_cid,
                           &parent,      &comp_min,    &sort_hist,   &scan_scratch, &small,      &hash_keys,
                           &hash_vals,   &nbr_list,    &jobs_dev,    &batch_bbox,  &cell_job,    &job_counters,
-                          &items_split, &col_range,   &ids_in};
+                          &items_split, &col_range,   &ids_in,      &batch_in,    &batch_nn,    &batch_ci,
+                          &load_box};
         for (DevBuf *b : bufs) f(*b);
     }
     size_t held_bytes() {
@@ -136,6 +150,14 @@ struct Fail {
 
 constexpr uint32_t kAllFlags = NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS |
                                NDB_FLAG_EXACT_COUNT | NDB_FLAG_TENSOR_FILTER | NDB_FLAG_FILTER_AUDIT;
+// internal: the job is the context's loaded copy (ndb_b200_run_loaded); never a caller's flag
+constexpr uint32_t kFlagLoaded = 0x80000000u;
+
+// load_box layout: lo_hi ints, then the invalid-point count, then two error words
+constexpr size_t kLoadBoxInvalidOff = 2 * kMaxDim * sizeof(int);
+constexpr size_t kLoadBoxErrOff = kLoadBoxInvalidOff + 8;
+constexpr size_t kLoadBoxBytes = kLoadBoxErrOff + 8;
+constexpr size_t kPinChunk = size_t(32) << 20;  // bytes of one pinned staging chunk
 
 inline void ck(ndb_ctx *ctx, cudaError_t e) {
     if (e == cudaSuccess) return;
@@ -159,6 +181,12 @@ inline void ensure(ndb_ctx *ctx, DevBuf &b, size_t bytes) { ck(ctx, grow(ctx, b,
 template <typename T>
 T *small_at(ndb_ctx *ctx, size_t off) {
     return reinterpret_cast<T *>(static_cast<char *>(ctx->small.ptr) + off);
+}
+
+// An event of the context, created on first use.
+inline cudaEvent_t lazy_event(ndb_ctx *ctx, cudaEvent_t &e) {
+    if (!e) ck(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return e;
 }
 
 // ---------------------------------------------------------------------------
@@ -830,21 +858,31 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ck(ctx, cudaMemsetAsync(ctx->small.ptr, 0, kSmallBytes, st));
     cudaEventRecord(ctx->ev[0], st);
 
-    if (flags & NDB_FLAG_DEVICE_PTRS) {
+    if (flags & kFlagLoaded) {
+        ctx->coords_dev = ctx->coords.as<float>();
+    } else if (flags & NDB_FLAG_DEVICE_PTRS) {
         ctx->coords_dev = coords;
     } else {
+        ctx->loaded = false;  // the loaded copy is overwritten
         ensure(ctx, ctx->coords, (size_t)n * D * sizeof(float));
         ck(ctx, cudaMemcpyAsync(ctx->coords.ptr, coords, (size_t)n * D * sizeof(float), cudaMemcpyHostToDevice, st));
         ctx->coords_dev = ctx->coords.as<float>();
     }
 
-    // bounding box of the grid-eligible points
+    // bounding box of the grid-eligible points (a loaded job's was reduced while it arrived)
     int *lo_hi = small_at<int>(ctx, kSmallBboxOff);
     unsigned long long *n_invalid = small_at<unsigned long long>(ctx, kSmallInvalidOff);
-    ++launch_counter(), bbox_init_kernel<<<1, 32, 0, st>>>(lo_hi, D, n_invalid, small_at<int>(ctx, kSmallErrOff),
-                                                           ctx->uf_max_steps);
-    ++launch_counter(), bbox_kernel<D><<<std::min<unsigned>(blocks_for(n), 148 * 8), kBlock, 0, st>>>(ctx->coords_dev, n, lo_hi,
-                                                                                  n_invalid);
+    if (flags & kFlagLoaded) {
+        ck(ctx, cudaMemcpyAsync(lo_hi, ctx->load_box.ptr, 2 * D * sizeof(int), cudaMemcpyDeviceToDevice, st));
+        ck(ctx, cudaMemcpyAsync(n_invalid, ctx->load_box.as<char>() + kLoadBoxInvalidOff, sizeof(unsigned long long),
+                                cudaMemcpyDeviceToDevice, st));
+        ++launch_counter(), set_int_kernel<<<1, 1, 0, st>>>(small_at<int>(ctx, kSmallErrOff) + 1, ctx->uf_max_steps);
+    } else {
+        ++launch_counter(), bbox_init_kernel<<<1, 32, 0, st>>>(lo_hi, D, n_invalid, small_at<int>(ctx, kSmallErrOff),
+                                                               ctx->uf_max_steps);
+        ++launch_counter(), bbox_kernel<D><<<std::min<unsigned>(blocks_for(n), 148 * 8), kBlock, 0, st>>>(
+            ctx->coords_dev, n, lo_hi, n_invalid);
+    }
     ck(ctx, cudaGetLastError());
     int h_lo_hi[2 * kMaxDim];
     unsigned long long h_invalid = 0;
@@ -992,6 +1030,98 @@ ndb_status labels_entry(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
     }
 }
 
+// The reference's binary input (magma_input.h:113-125): int32 n, int32 d, then
+// n*d float32 row-major.  Read in chunks into two pinned buffers; chunk k's copy to
+// the device runs on the copy stream while chunk k+1 is read from the file, and the
+// bounding-box kernel reduces chunk k on the context's stream as soon as it landed.
+template <int D>
+void bbox_chunk(ndb_ctx *ctx, const float *p, int64_t cnt) {
+    int *lo_hi = ctx->load_box.as<int>();
+    auto *inval = reinterpret_cast<unsigned long long *>(ctx->load_box.as<char>() + kLoadBoxInvalidOff);
+    ++launch_counter(), bbox_kernel<D><<<std::min<unsigned>(blocks_for(cnt), 148 * 8), kBlock, 0, ctx->stream>>>(
+        p, cnt, lo_hi, inval);
+    ck(ctx, cudaGetLastError());
+}
+
+ndb_status load_bin_impl(ndb_ctx *ctx, FILE *f, int64_t *n_out, int32_t *d_out) {
+    int32_t hdr[2];
+    if (fread(hdr, sizeof(int32_t), 2, f) != 2) return NDB_ERR_IO;
+    const int64_t n = hdr[0];
+    const int d = hdr[1];
+    if (n < 0) return NDB_ERR_IO;
+    if (d < 1 || d > NDB_MAX_DIM) return NDB_ERR_UNSUPPORTED_DIM;
+    if (fseeko(f, 0, SEEK_END) != 0) return NDB_ERR_IO;
+    const off_t size = ftello(f);
+    if (size < (off_t)(8 + n * d * (int64_t)sizeof(float)) || fseeko(f, 8, SEEK_SET) != 0) return NDB_ERR_IO;
+    cudaStream_t st = ctx->stream;
+    ensure(ctx, ctx->coords, (size_t)(n * d + 1) * sizeof(float));
+    ensure(ctx, ctx->load_box, kLoadBoxBytes);
+    if (ctx->pin_bytes < kPinChunk) {
+        for (int b = 0; b < 2; ++b) {
+            if (ctx->pin[b]) cudaFreeHost(ctx->pin[b]);
+            ctx->pin[b] = nullptr;
+        }
+        ctx->pin_bytes = 0;
+        for (int b = 0; b < 2; ++b) ck(ctx, cudaHostAlloc(&ctx->pin[b], kPinChunk, cudaHostAllocDefault));
+        ctx->pin_bytes = kPinChunk;
+    }
+    for (int b = 0; b < 2; ++b) lazy_event(ctx, ctx->ev_pin[b]);
+    ++launch_counter(), bbox_init_kernel<<<1, 32, 0, st>>>(
+        ctx->load_box.as<int>(), d, reinterpret_cast<unsigned long long *>(ctx->load_box.as<char>() + kLoadBoxInvalidOff),
+        reinterpret_cast<int *>(ctx->load_box.as<char>() + kLoadBoxErrOff), 0);
+    ck(ctx, cudaGetLastError());
+    const int64_t per = (int64_t)(ctx->pin_bytes / (sizeof(float) * d));
+    int k = 0;
+    for (int64_t off = 0; off < n; off += per, ++k) {
+        const int b = k & 1;
+        const int64_t cnt = std::min(per, n - off);
+        if (k >= 2) ck(ctx, cudaEventSynchronize(ctx->ev_pin[b]));  // the buffer's previous copy is done
+        if (fread(ctx->pin[b], sizeof(float) * d, (size_t)cnt, f) != (size_t)cnt) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            return NDB_ERR_IO;
+        }
+        float *dst = ctx->coords.as<float>() + off * d;
+        ck(ctx, cudaMemcpyAsync(dst, ctx->pin[b], (size_t)cnt * d * sizeof(float), cudaMemcpyHostToDevice,
+                                ctx->copy_stream));
+        ck(ctx, cudaEventRecord(ctx->ev_pin[b], ctx->copy_stream));
+        ck(ctx, cudaStreamWaitEvent(st, ctx->ev_pin[b], 0));
+        switch (d) {
+            case 1: bbox_chunk<1>(ctx, dst, cnt); break;
+            case 2: bbox_chunk<2>(ctx, dst, cnt); break;
+            case 3: bbox_chunk<3>(ctx, dst, cnt); break;
+            case 4: bbox_chunk<4>(ctx, dst, cnt); break;
+            case 5: bbox_chunk<5>(ctx, dst, cnt); break;
+            case 6: bbox_chunk<6>(ctx, dst, cnt); break;
+            case 7: bbox_chunk<7>(ctx, dst, cnt); break;
+            case 8: bbox_chunk<8>(ctx, dst, cnt); break;
+            case 9: bbox_chunk<9>(ctx, dst, cnt); break;
+            case 10: bbox_chunk<10>(ctx, dst, cnt); break;
+            case 11: bbox_chunk<11>(ctx, dst, cnt); break;
+            case 12: bbox_chunk<12>(ctx, dst, cnt); break;
+            case 13: bbox_chunk<13>(ctx, dst, cnt); break;
+            case 14: bbox_chunk<14>(ctx, dst, cnt); break;
+            case 15: bbox_chunk<15>(ctx, dst, cnt); break;
+            default: bbox_chunk<16>(ctx, dst, cnt); break;
+        }
+    }
+    // the pinned buffers are reused by the next load: its first reads wait on these copies
+    ctx->loaded = true;
+    ctx->loaded_n = n;
+    ctx->loaded_d = d;
+    *n_out = n;
+    *d_out = d;
+    return NDB_OK;
+}
+
+ndb_status load_bin_file(ndb_ctx *ctx, FILE *f, int64_t *n_out, int32_t *d_out) {
+    try {
+        return load_bin_impl(ctx, f, n_out, d_out);
+    } catch (const Fail &fl) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        return fl.st;
+    }
+}
+
 // ndb_b200_assign_border: the border pass again, with the caller's ids for the cores.
 template <int D>
 ndb_status border_ids_impl(ndb_ctx *ctx, const int32_t *core_ids, int32_t *ci_out) {
@@ -1110,6 +1240,13 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
     for (auto &e : ctx->kev)
         if (e) cudaEventDestroy(e);
     if (ctx->ev_nn) cudaEventDestroy(ctx->ev_nn);
+    for (auto &e : ctx->ev_grp)
+        if (e) cudaEventDestroy(e);
+    if (ctx->ev_out) cudaEventDestroy(ctx->ev_out);
+    for (int b = 0; b < 2; ++b) {
+        if (ctx->ev_pin[b]) cudaEventDestroy(ctx->ev_pin[b]);
+        if (ctx->pin[b]) cudaFreeHost(ctx->pin[b]);
+    }
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -1165,19 +1302,20 @@ ndb_status ndb_b200_set_stream(ndb_ctx *ctx, void *stream) {
     return NDB_OK;
 }
 
-ndb_status ndb_b200_classify(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
-                             uint32_t flags, int32_t *nn_out) {
+// ndb_b200_classify with the internal flag allowed (the loaded job).
+static ndb_status classify_checked(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps,
+                                   int32_t min_pts, uint32_t flags, int32_t *nn_out) {
     ndb_status s = check_ctx(ctx);
     if (s != NDB_OK) return s;
-    if (flags & ~kAllFlags) return NDB_ERR_INVALID_ARGUMENT;
+    if (flags & ~(kAllFlags | kFlagLoaded)) return NDB_ERR_INVALID_ARGUMENT;
     if (n < 0) return NDB_ERR_INVALID_ARGUMENT;
     if (n > NDB_MAX_POINTS) return NDB_ERR_TOO_MANY_POINTS;
     if (d < 1 || d > NDB_MAX_DIM) return NDB_ERR_UNSUPPORTED_DIM;
-    if (n > 0 && !coords) return NDB_ERR_INVALID_ARGUMENT;
+    if (n > 0 && !coords && !(flags & kFlagLoaded)) return NDB_ERR_INVALID_ARGUMENT;
     const float e2 = eps * eps;
     if (!isfinite(e2)) return NDB_ERR_INVALID_EPS;
     if ((flags & NDB_FLAG_DEVICE_PTRS) && n > 0) {
-        if (!is_device_ptr(coords)) return NDB_ERR_INVALID_ARGUMENT;
+        if (!(flags & kFlagLoaded) && !is_device_ptr(coords)) return NDB_ERR_INVALID_ARGUMENT;
         if (nn_out && !is_device_ptr(nn_out)) return NDB_ERR_INVALID_ARGUMENT;
     }
     if (n == 0) {
@@ -1198,6 +1336,12 @@ ndb_status ndb_b200_classify(ndb_ctx *ctx, const float *coords, int64_t n, int32
 #undef NDB_CLASSIFY
 }
 
+ndb_status ndb_b200_classify(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
+                             uint32_t flags, int32_t *nn_out) {
+    if (flags & kFlagLoaded) return NDB_ERR_INVALID_ARGUMENT;
+    return classify_checked(ctx, coords, n, d, eps, min_pts, flags, nn_out);
+}
+
 ndb_status ndb_b200_assign_labels(ndb_ctx *ctx, int32_t *cluster_index_out, ndb_result *result) {
     ndb_status s = check_ctx(ctx);
     if (s != NDB_OK) return s;
@@ -1216,11 +1360,11 @@ ndb_status ndb_b200_assign_labels(ndb_ctx *ctx, int32_t *cluster_index_out, ndb_
 #undef NDB_LABELS
 }
 
-ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
-                        uint32_t flags, int32_t *nn_out, int32_t *cluster_index_out, ndb_result *result) {
+static ndb_status run_checked(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
+                              uint32_t flags, int32_t *nn_out, int32_t *cluster_index_out, ndb_result *result) {
     if (!ctx) return NDB_ERR_INVALID_ARGUMENT;
     ctx->in_run = true;
-    ndb_status s = ndb_b200_classify(ctx, coords, n, d, eps, min_pts, flags, nn_out);
+    ndb_status s = classify_checked(ctx, coords, n, d, eps, min_pts, flags, nn_out);
     ctx->in_run = false;
     if (s == NDB_OK) s = ndb_b200_assign_labels(ctx, cluster_index_out, result);
     if (ctx->nn_pending) {
@@ -1230,6 +1374,35 @@ ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d,
         if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && s == NDB_OK) s = NDB_ERR_CUDA;
     }
     return s;
+}
+
+ndb_status ndb_b200_run(ndb_ctx *ctx, const float *coords, int64_t n, int32_t d, float eps, int32_t min_pts,
+                        uint32_t flags, int32_t *nn_out, int32_t *cluster_index_out, ndb_result *result) {
+    if (flags & kFlagLoaded) return NDB_ERR_INVALID_ARGUMENT;
+    return run_checked(ctx, coords, n, d, eps, min_pts, flags, nn_out, cluster_index_out, result);
+}
+
+ndb_status ndb_b200_load_bin(ndb_ctx *ctx, const char *path, int64_t *n_out, int32_t *d_out) {
+    ndb_status s = check_ctx(ctx);
+    if (s != NDB_OK) return s;
+    if (!path || !n_out || !d_out) return NDB_ERR_INVALID_ARGUMENT;
+    ctx->loaded = false;
+    ctx->have_state = false;
+    ctx->have_labels = false;
+    FILE *f = fopen(path, "rb");
+    if (!f) return NDB_ERR_IO;
+    s = load_bin_file(ctx, f, n_out, d_out);
+    fclose(f);
+    return s;
+}
+
+ndb_status ndb_b200_run_loaded(ndb_ctx *ctx, float eps, int32_t min_pts, uint32_t flags, int32_t *nn_out,
+                               int32_t *cluster_index_out, ndb_result *result) {
+    if (!ctx) return NDB_ERR_INVALID_ARGUMENT;
+    if (!ctx->loaded) return NDB_ERR_NO_STATE;
+    if (flags & ~kAllFlags) return NDB_ERR_INVALID_ARGUMENT;
+    return run_checked(ctx, ctx->coords.as<float>(), ctx->loaded_n, ctx->loaded_d, eps, min_pts, flags | kFlagLoaded,
+                       nn_out, cluster_index_out, result);
 }
 
 ndb_status ndb_b200_cluster_label(ndb_ctx *ctx, int32_t *label_out, int64_t capacity) {
@@ -1287,6 +1460,7 @@ const char *ndb_b200_strerror(ndb_status s) {
         case NDB_ERR_DEVICE_LIMIT: return "device-side iteration bound reached";
         case NDB_ERR_NO_STATE: return "no classified job in this context";
         case NDB_ERR_BAD_JOB: return "invalid batched job descriptor";
+        case NDB_ERR_IO: return "cannot read the input file (missing, short, or a bad header)";
     }
     return "unknown status";
 }
@@ -1768,6 +1942,60 @@ ndb_status run_group_entry(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &
     }
 }
 
+// Host buffers of a batched run: every job's coordinates go to the device on the
+// copy stream, group after group in the order the groups run, with an event per
+// group; the jobs the pipelines see (dj) point at the device copies and at device
+// output slots.  Later groups' copies then overlap earlier groups' compute.
+void stage_batch(ndb_ctx *ctx, const ndb_job *jobs, int64_t n_jobs, const std::vector<std::vector<int>> &groups,
+                 std::vector<ndb_job> &dj) {
+    size_t nf = 0, np = 0;
+    bool want_nn = false, want_ci = false;
+    for (int d = 1; d <= NDB_MAX_DIM; ++d)
+        for (int i : groups[d]) {
+            nf += (size_t)jobs[i].n * d;
+            np += (size_t)jobs[i].n;
+            want_nn |= jobs[i].nn_out != nullptr;
+            want_ci |= jobs[i].cluster_index_out != nullptr;
+        }
+    ensure(ctx, ctx->batch_in, (nf + 4) * sizeof(float));
+    if (want_nn) ensure(ctx, ctx->batch_nn, (np + 1) * sizeof(int32_t));
+    if (want_ci) ensure(ctx, ctx->batch_ci, (np + 1) * sizeof(int32_t));
+    dj.assign(jobs, jobs + n_jobs);
+    size_t f = 0, p = 0;
+    for (int d = 1; d <= NDB_MAX_DIM; ++d) {
+        if (groups[d].empty()) continue;
+        for (int i : groups[d]) {
+            const ndb_job &J = jobs[i];
+            float *dst = ctx->batch_in.as<float>() + f;
+            ck(ctx, cudaMemcpyAsync(dst, J.coords, (size_t)J.n * d * sizeof(float), cudaMemcpyHostToDevice,
+                                    ctx->copy_stream));
+            dj[i].coords = dst;
+            dj[i].nn_out = J.nn_out ? ctx->batch_nn.as<int32_t>() + p : nullptr;
+            dj[i].cluster_index_out = J.cluster_index_out ? ctx->batch_ci.as<int32_t>() + p : nullptr;
+            f += (size_t)J.n * d;
+            p += (size_t)J.n;
+        }
+        ck(ctx, cudaEventRecord(lazy_event(ctx, ctx->ev_grp[d]), ctx->copy_stream));
+    }
+}
+
+// Outputs of finished jobs back to the caller's buffers on the copy stream, after
+// the work queued so far on the context's stream: they overlap what comes next.
+void unstage_jobs(ndb_ctx *ctx, const ndb_job *jobs, const std::vector<ndb_job> &dj, const std::vector<int> &which) {
+    if (which.empty()) return;
+    ck(ctx, cudaEventRecord(lazy_event(ctx, ctx->ev_out), ctx->stream));
+    ck(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_out, 0));
+    for (int i : which) {
+        const ndb_job &J = jobs[i];
+        if (J.nn_out)
+            ck(ctx, cudaMemcpyAsync(J.nn_out, dj[i].nn_out, (size_t)J.n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                    ctx->copy_stream));
+        if (J.cluster_index_out)
+            ck(ctx, cudaMemcpyAsync(J.cluster_index_out, dj[i].cluster_index_out, (size_t)J.n * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, ctx->copy_stream));
+    }
+}
+
 }  // namespace
 
 extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t n_jobs, uint32_t flags) {
@@ -1803,8 +2031,28 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
         if (J.n == 0) continue;
         groups[J.d].push_back((int)i);
     }
+    // host buffers: inputs staged group by group on the copy stream, outputs back
+    // group by group; the pipelines run on the device copies
+    const bool host_io = !(flags & NDB_FLAG_DEVICE_PTRS) && ctx->copy_stream;
+    std::vector<ndb_job> dj;
+    ndb_job *work = jobs;
+    uint32_t wflags = flags;
+    if (host_io) {
+        try {
+            stage_batch(ctx, jobs, n_jobs, groups, dj);
+        } catch (const Fail &f) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            return f.st;
+        }
+        work = dj.data();
+        wflags |= NDB_FLAG_DEVICE_PTRS;
+    }
     std::vector<int> solo;
     for (int d = 1; d <= NDB_MAX_DIM; ++d) {
+        if (host_io && !groups[d].empty() && cudaStreamWaitEvent(ctx->stream, ctx->ev_grp[d], 0) != cudaSuccess) {
+            if (first == NDB_OK) first = NDB_ERR_CUDA;
+        }
+        const size_t solo_before = solo.size();
         // pipelines of at most kMaxBatchPoints points
         size_t b = 0;
         while (b < groups[d].size()) {
@@ -1814,7 +2062,7 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
                 pts += jobs[groups[d][b]].n;
                 members.push_back(groups[d][b++]);
             }
-#define NDB_GROUP(D) run_group_entry<D>(ctx, jobs, members, flags, solo)
+#define NDB_GROUP(D) run_group_entry<D>(ctx, work, members, wflags, solo)
             ndb_status gs;
             switch (d) {
                 case 1: gs = NDB_GROUP(1); break;
@@ -1837,15 +2085,25 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
 #undef NDB_GROUP
             if (gs != NDB_OK && first == NDB_OK) first = gs;
         }
+        if (host_io && !groups[d].empty()) {
+            std::vector<int> done;
+            for (int i : groups[d])
+                if (std::find(solo.begin() + solo_before, solo.end(), i) == solo.end()) done.push_back(i);
+            try {
+                unstage_jobs(ctx, jobs, dj, done);
+            } catch (const Fail &f) {
+                if (first == NDB_OK) first = f.st;
+            }
+        }
     }
     // statistics of the pipelines, then of the jobs the pipelines could not take,
     // which run one call each
     ndb_stats acc = ctx->stats;
     acc.kernel_launches = launch_counter();
     for (int i : solo) {
-        ndb_job &J = jobs[i];
+        ndb_job &J = work[i];
         ndb_result r{};
-        const ndb_status js = ndb_b200_run(ctx, J.coords, J.n, J.d, J.eps, J.min_pts, flags, J.nn_out,
+        const ndb_status js = ndb_b200_run(ctx, J.coords, J.n, J.d, J.eps, J.min_pts, wflags, J.nn_out,
                                            J.cluster_index_out, &r);
         J.status = js;
         if (js == NDB_OK) J.result = r;
@@ -1877,6 +2135,18 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     }
     acc.solo_jobs = (int32_t)solo.size();
     ctx->stats = acc;
+    if (host_io) {
+        try {
+            unstage_jobs(ctx, jobs, dj, solo);
+        } catch (const Fail &f) {
+            if (first == NDB_OK) first = f.st;
+        }
+        if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && first == NDB_OK) first = NDB_ERR_CUDA;
+        for (int64_t i = 0; i < n_jobs; ++i) {
+            jobs[i].status = dj[i].status;
+            jobs[i].result = dj[i].result;
+        }
+    }
     // a pipeline reports a device-side failure through its jobs' statuses
     for (int64_t i = 0; i < n_jobs && first == NDB_OK; ++i)
         if (jobs[i].status != NDB_OK) first = (ndb_status)jobs[i].status;

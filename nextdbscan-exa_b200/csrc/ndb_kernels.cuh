@@ -1224,7 +1224,23 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) union_points_kernel(
         int tested = 0;
         for (int k = 0; k < nc; ++k) {
             const int ik = sidx[k];
-            if (valid && j > ik && sroot[k] != pj) {
+            if constexpr (D >= 8) {
+                // as in the count: the second half of the sum only when some lane's
+                // first half is still within e2 (exact: partial sums only grow)
+                const bool want = valid && j > ik && sroot[k] != pj;
+                if (!__any_sync(kFull, want)) continue;
+                float xi[D];
+                load_point_smem<D>(si + k * P, xi);
+                constexpr int H = D / 2;
+                const float len = dist_part<D, 0, H>(xi, xj, 0.0f);
+                bool hit = false;
+                if (__any_sync(kFull, want && len <= e2)) hit = want && dist_part<D, H, D>(xi, xj, len) <= e2;
+                tested += want ? 1 : 0;
+                if (hit) {
+                    uf_union(parent, ik, j, err);
+                    pj = uf_find(parent, j, err);
+                }
+            } else if (valid && j > ik && sroot[k] != pj) {
                 float xi[D];
                 load_point_smem<D>(si + k * P, xi);
                 ++tested;

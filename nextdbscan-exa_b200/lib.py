@@ -34,6 +34,7 @@ STATUS = {
     8: "NDB_ERR_DEVICE_LIMIT",
     9: "NDB_ERR_NO_STATE",
     10: "NDB_ERR_BAD_JOB",
+    11: "NDB_ERR_IO",
 }
 
 # Every symbol include/ndb_b200.h declares (tests check the library exports them).
@@ -44,6 +45,8 @@ EXPORTED = (
     "ndb_b200_classify",
     "ndb_b200_assign_labels",
     "ndb_b200_run",
+    "ndb_b200_load_bin",
+    "ndb_b200_run_loaded",
     "ndb_b200_run_batched",
     "ndb_b200_cluster_label",
     "ndb_b200_assign_border",
@@ -159,6 +162,10 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
                                      ctypes.c_float, ctypes.c_int32, ctypes.c_uint32, i32p, i32p,
                                      ctypes.POINTER(NdbResult)]
+        lib.ndb_b200_load_bin.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.POINTER(ctypes.c_int32)]
+        lib.ndb_b200_run_loaded.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_int32, ctypes.c_uint32, i32p,
+                                            i32p, ctypes.POINTER(NdbResult)]
         lib.ndb_b200_run_batched.argtypes = [ctypes.c_void_p, ctypes.POINTER(NdbJob), ctypes.c_int64,
                                              ctypes.c_uint32]
         lib.ndb_b200_cluster_label.argtypes = [ctypes.c_void_p, i32p, ctypes.c_int64]
@@ -176,7 +183,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         lib.ndb_b200_version.restype = ctypes.c_char_p
         for name in ("ndb_b200_create", "ndb_b200_destroy", "ndb_b200_set_stream", "ndb_b200_classify",
                      "ndb_b200_assign_labels", "ndb_b200_run", "ndb_b200_run_batched", "ndb_b200_cluster_label",
-                     "ndb_b200_assign_border",
+                     "ndb_b200_assign_border", "ndb_b200_load_bin", "ndb_b200_run_loaded",
                      "ndb_b200_get_stats", "ndb_b200_set_memory_limit", "ndb_b200_device_bytes",
                      "ndb_b200_set_tuning", "ndb_b200_get_tuning", "ndb_b200_set_debug_limits"):
             getattr(lib, name).restype = ctypes.c_int
