@@ -740,7 +740,9 @@ def roofline(kind, ms, s, n, hbm_peak, peak_src, clk):
              "border_kernel": s["border_pairs"]}[kind]
     pair_dims = {"count_kernel": s["count_pair_dims"], "union_kernel": s["union_pair_dims"],
                  "border_kernel": s["border_pair_dims"]}[kind]
-    flops = pair_dims * 3  # separately rounded sub, mul, add per dimension (no FMA credit)
+    # FP32 pipe operations: the exact sum takes a separately rounded sub, mul and add per
+    # dimension (no FMA credit); the Gram filter one FMA per dimension plus three
+    flops = s.get("count_fp32_ops") if kind == "count_kernel" and s.get("count_fp32_ops") else pair_dims * 3
     achieved = flops / (ms / 1000.0) / 1e12
     mhz = clk.get("sm_mhz") or 1965.0
     peak = SM_COUNT * FP32_LANES_PER_SM * mhz * 1e6 / 1e12
@@ -748,7 +750,7 @@ def roofline(kind, ms, s, n, hbm_peak, peak_src, clk):
             "frac": achieved / peak, "traffic": None,
             "peak_source": "nominal FP32 issue rate (148 SMs x 128 lanes) at the median sampled SM clock; "
                            "no FP32 figure in MEASURED_PEAKS.json",
-            "work": f"{pairs} pair predicates x 3d FP32 ops"}
+            "work": f"{pairs} pair predicates, {flops} FP32 pipe operations"}
 
 
 def main():

@@ -72,8 +72,8 @@ typedef enum ndb_status {
                                       upper bound on the cluster count. */
 #define NDB_FLAG_FULL_COUNT  0x2u  /* exact nn for every point (no early exit at min_pts) */
 #define NDB_FLAG_DEVICE_PTRS 0x4u  /* coords and outputs are device pointers */
-#define NDB_FLAG_EXACT_COUNT 0x8u  /* count with the exact FP32 kernel only, never the tensor-core
-                                    * filter (results are identical either way; this is the plain form) */
+#define NDB_FLAG_EXACT_COUNT 0x8u  /* count with the exact FP32 kernel only, never the tensor-core or the
+                                    * FP32 Gram filter (results are identical either way; this is the plain form) */
 #define NDB_FLAG_TENSOR_FILTER 0x10u /* d >= 8: count on the tensor-core filter whenever the input allows
                                       * it, whatever the tile-fill heuristic would pick (results identical) */
 #define NDB_FLAG_FILTER_AUDIT 0x20u  /* diagnostic: when the tensor-core filter runs, measure every pair it
@@ -113,7 +113,7 @@ typedef struct ndb_stats {
     int32_t key_bytes;        /* 4 or 8 */
     int32_t kernel_launches;  /* kernels launched by the last classify + assign_labels */
     int32_t pipelines;        /* batched runs: pipelines built (one per d and chunk of jobs) */
-    int64_t count_pair_dims;  /* dimensions evaluated by the count, summed over pipelines (3 FP32 operations each) */
+    int64_t count_pair_dims;  /* sum over pipelines of count_pairs x d */
     int64_t union_pair_dims;  /* the same for the union-find */
     int64_t border_pair_dims; /* the same for the border assignment */
     int32_t solo_jobs;        /* batched runs: jobs the pipelines could not take, run one call each */
@@ -126,8 +126,9 @@ typedef struct ndb_stats {
     double filter_max_err_over_bound; /* largest |D~ - d64| over the error bound the guard band is built from */
     int64_t filter_audited_pairs;     /* pairs measured */
     int64_t filter_misclassified_pairs; /* pairs decided outside the band that the exact predicate decides otherwise */
-    int64_t count_skipped_dims;       /* pair dimensions the exact count never evaluated (d >= 8: a warp whose
-                                       * partial sums all passed eps^2 skips the rest; count_pair_dims excludes them) */
+    int64_t count_fp32_ops;           /* FP32 pipe operations of the CUDA-core count: 3d per pair for the exact
+                                       * sum, d + 3 per pair with the Gram filter (one FMA per dimension) */
+    int32_t gram_filter;              /* 1 when the CUDA-core count ran with the Gram filter (d >= 8) */
 } ndb_stats;
 
 typedef struct ndb_ctx ndb_ctx;

@@ -48,6 +48,7 @@ struct ndb_ctx {
     size_t list_budget = size_t(8) << 30;  // largest list buffer the context may use (else: scan border)
     int list_cap = 0;                 // entries per point, 0 when the lists are off
     bool tc_count = false;            // neighbour count on the tensor-core filter
+    bool gram_count = false;          // CUDA-core count with the Gram filter (d >= 8)
     int sm_count = 148;
     // scratch
     DevBuf sort_hist, scan_scratch, small;  // small: counters, bbox, scalars
@@ -127,7 +128,6 @@ constexpr size_t kSmallBboxOff = 0;          // int[2*kMaxDim]
 constexpr size_t kSmallInvalidOff = 256;     // u64
 constexpr size_t kSmallCountersOff = 512;    // u64[12]: 0 clusters 1 noise 2 count pairs 3 union pairs 4 border pairs
                                              // 5 band pairs 6 work counter of the persistent count kernel
-                                             // 7 pair dimensions the count skipped (partial sums past e2)
                                              // 8..11 filter audit (tc::audit_tile)
 constexpr int kCounters = 12;
 constexpr size_t kSmallScalarOff = 1024;     // u32[8]: 0 n_cells 1 n_items 2 n_cores
@@ -516,6 +516,18 @@ inline bool tc_eligible(const ndb_ctx *ctx, int d, float e2, const double *lo, c
     return true;
 }
 
+// The Gram-filtered count on CUDA cores (count_kernel<D, E, true>): d >= 8, not the
+// plain form (NDB_FLAG_EXACT_COUNT), eps^2 a normal float far from under- and
+// overflow, and coordinates within +-2^60 so that no centred square or norm
+// overflows.  Results never depend on it.
+inline bool gram_eligible(int d, float e2, const double *lo, const double *hi, uint32_t flags) {
+    if (d < 8 || (flags & NDB_FLAG_EXACT_COUNT)) return false;
+    if (!(e2 >= 0x1p-100f && e2 <= 0x1p100f)) return false;
+    for (int a = 0; a < d; ++a)
+        if (!(fabs(lo[a]) <= 0x1p60 && fabs(hi[a]) <= 0x1p60)) return false;
+    return true;
+}
+
 // Which items the tensor kernel takes: it stages every candidate row once per item
 // and most of its per-tile epilogue is fixed, so it pays only for full items (many
 // points of one cell).  Measured on B200: with about 11 points per item the exact
@@ -567,7 +579,7 @@ void launch_count_tc(ndb_ctx *ctx, int64_t n_items, const int2 *items, const int
 // eligible); then the items are split by size and each list goes to its kernel,
 // both launched at the upper bound and reading their list length on the device.
 template <int D>
-void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_items, const int2 *items,
+void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool gram, bool early, int64_t n_items, const int2 *items,
                  const int32_t *cell_start, const int2 *nbr, int n_rows, const float *xs, float e2, int min_pts,
                  int dense_skip, int32_t *nn_sorted, int32_t *list, int list_cap, int list_stride,
                  const JobDev *jobs, const int32_t *cell_job, bool audit) {
@@ -591,14 +603,25 @@ void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool early, int64_t n_ite
         ex_n = scal + 5;
     }
     const unsigned grid = (unsigned)((n_items + kCountWarps - 1) / kCountWarps);
-    if (early)
-        ++launch_counter(), count_kernel<D, true><<<grid, kCountWarps * kWarp, 0, st>>>(
+    // the counts on CUDA cores: the Gram-filtered kernel (d >= 8) or the exact one
+    auto launch = [&](auto early_c, auto gram_c) {
+        constexpr bool E = decltype(early_c)::value, G = decltype(gram_c)::value;
+        ++launch_counter(), count_kernel<D, E, G><<<grid, kCountWarps * kWarp, 0, st>>>(
             ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
-            list_stride, counters + 2, jobs, cell_job, ex_n, counters + 7);
-    else
-        ++launch_counter(), count_kernel<D, false><<<grid, kCountWarps * kWarp, 0, st>>>(
-            ex_items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, dense_skip, nn_sorted, list, list_cap,
-            list_stride, counters + 2, jobs, cell_job, ex_n, counters + 7);
+            list_stride, counters + 2, jobs, cell_job, ex_n, counters + 5);
+    };
+    using T = std::true_type;
+    using F = std::false_type;
+    if constexpr (D >= 8) {
+        if (gram) {
+            if (early) launch(T{}, T{});
+            else launch(F{}, T{});
+            ck(ctx, cudaGetLastError());
+            return;
+        }
+    }
+    if (early) launch(T{}, F{});
+    else launch(F{}, F{});
     ck(ctx, cudaGetLastError());
 }
 
@@ -617,7 +640,8 @@ void count_phase(ndb_ctx *ctx) {
     }
     int32_t *list = ctx->list_cap ? ctx->nbr_list.as<int32_t>() : nullptr;
     cudaEventRecord(ctx->kev[2], st);
-    count_items<D>(ctx, ctx->tc_count, (ctx->flags_run & NDB_FLAG_TENSOR_FILTER) != 0, early, ctx->n_items,
+    count_items<D>(ctx, ctx->tc_count, (ctx->flags_run & NDB_FLAG_TENSOR_FILTER) != 0, ctx->gram_count, early,
+                   ctx->n_items,
                    ctx->items.as<int2>(), ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows,
                    ctx->xs.as<float>(), ctx->e2, ctx->min_pts, ctx->cell_units, ctx->nn_sorted.as<int32_t>(), list,
                    ctx->list_cap, ctx->list_cap, nullptr, nullptr, (ctx->flags_run & NDB_FLAG_FILTER_AUDIT) != 0);
@@ -830,8 +854,9 @@ void classify_stats(ndb_ctx *ctx) {
     ck(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->stats.tensor_items = ctx->tc_count ? h_tc_items : 0;
     ctx->stats.count_pairs = (int64_t)h_counters[2];
-    ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D - (int64_t)h_counters[7];
-    ctx->stats.count_skipped_dims = (int64_t)h_counters[7];
+    ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
+    ctx->stats.count_fp32_ops = (int64_t)h_counters[2] * (ctx->gram_count ? D + 3 : 3 * D);
+    ctx->stats.gram_filter = ctx->gram_count ? 1 : 0;
     ctx->stats.band_pairs = (int64_t)h_counters[5];
     audit_stats(ctx->stats, h_counters + 8);
     ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
@@ -908,6 +933,7 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->cell_units = pl.cell_units ? 1 : 0;
     if (pl.st.n_rows > kWarp) return NDB_ERR_INVALID_ARGUMENT;  // row tables hold one row per lane
     ctx->tc_count = tc_eligible(ctx, D, ctx->e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
+    ctx->gram_count = gram_eligible(D, ctx->e2, lo, hi, flags);
 
     classify_dispatch<D>(ctx, pl);
 
@@ -981,8 +1007,9 @@ ndb_status labels_impl(ndb_ctx *ctx, int32_t *ci_out, ndb_result *result) {
         ctx->stats_pending = false;
         ctx->stats.tensor_items = ctx->tc_count ? h_scal[4] : 0;
         ctx->stats.count_pairs = (int64_t)h_counters[2];
-        ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D - (int64_t)h_counters[7];
-        ctx->stats.count_skipped_dims = (int64_t)h_counters[7];
+        ctx->stats.count_pair_dims = (int64_t)h_counters[2] * D;
+        ctx->stats.count_fp32_ops = (int64_t)h_counters[2] * (ctx->gram_count ? D + 3 : 3 * D);
+        ctx->stats.gram_filter = ctx->gram_count ? 1 : 0;
         ctx->stats.band_pairs = (int64_t)h_counters[5];
         audit_stats(ctx->stats, h_counters + 8);
         ctx->stats.ms_grid = elapsed(ctx->ev[0], ctx->ev[1]);
@@ -1485,6 +1512,7 @@ struct BatchPlan {
     int linked = 0;
     int list_stride = 0;
     bool tc = false;  // neighbour count on the tensor-core filter (every job eligible)
+    bool gram = true; // CUDA-core count with the Gram filter (every job eligible)
     int64_t total_n = 0, nv = 0;
     double columns = 0;  // entries of the pipeline's column table (sum over its jobs)
 };
@@ -1597,7 +1625,8 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     const bool early = (flags & NDB_FLAG_FULL_COUNT) == 0;
     cudaEventRecord(ctx->ev[1], st);
     cudaEventRecord(ctx->kev[2], st);
-    count_items<D>(ctx, bp.tc, (flags & NDB_FLAG_TENSOR_FILTER) != 0, early, n_items, ctx->items.as<int2>(),
+    count_items<D>(ctx, bp.tc, (flags & NDB_FLAG_TENSOR_FILTER) != 0, bp.gram, early, n_items,
+                   ctx->items.as<int2>(),
                    ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows, ctx->xs.as<float>(), 0.0f, 0, 0,
                    ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, jobs_dev, cell_job,
                    (flags & NDB_FLAG_FILTER_AUDIT) != 0);
@@ -1705,14 +1734,12 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     std::vector<unsigned long long> h_jc((size_t)4 * nj);
     unsigned long long h_pairs[4] = {0, 0, 0, 0};  // count, union, border, band pairs (running totals)
     unsigned long long h_audit[4] = {0, 0, 0, 0};  // filter audit (running over the call's pipelines)
-    unsigned long long h_skipped = 0;              // pair dimensions the count skipped (running total)
     uint32_t h_tc_items = 0;
     int h_err = 0;
     if (bp.tc)
         ck(ctx, cudaMemcpyAsync(&h_tc_items, scal + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_pairs, counters + 2, sizeof(h_pairs), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_audit, counters + 8, sizeof(h_audit), cudaMemcpyDeviceToHost, st));
-    ck(ctx, cudaMemcpyAsync(&h_skipped, counters + 7, sizeof(h_skipped), cudaMemcpyDeviceToHost, st));
     ck(ctx, cudaMemcpyAsync(h_jc.data(), jc, (size_t)4 * nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             st));
     ck(ctx, cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1742,8 +1769,9 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     S.count_pairs += dc;
     S.union_pairs += du;
     S.border_pairs += db;
-    S.count_pair_dims += dc * D - ((int64_t)h_skipped - S.count_skipped_dims);
-    S.count_skipped_dims = (int64_t)h_skipped;
+    S.count_pair_dims += dc * D;
+    S.count_fp32_ops += dc * (bp.gram ? D + 3 : 3 * D);
+    S.gram_filter |= bp.gram ? 1 : 0;
     S.union_pair_dims += du * D;
     S.border_pair_dims += db * D;
     S.n_valid += nv;
@@ -1851,6 +1879,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
         }
         const Plan pl = plan_grid(D, jd.e2, lo, hi);
         const bool job_tc = tc_eligible(ctx, D, jd.e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
+        const bool job_gram = gram_eligible(D, jd.e2, lo, hi, flags);
         double cells = 1;
         for (int a = 0; a < pl.g.k; ++a) cells *= (double)pl.g.g[a];
         bool keep = (pl.cell_units ? 1 : 0) == bp.linked && jd.min_pts - 1 <= kMaxListCap &&
@@ -1861,6 +1890,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
             continue;
         }
         kept.push_back(members[m]);
+        bp.gram = bp.gram && job_gram;
         if (!have_stencil) {
             bp.st = pl.st;
             bp.tc = job_tc;
@@ -2119,7 +2149,8 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
         acc.tensor_items += s1.tensor_items;
         acc.tensor_filter |= s1.tensor_filter;
         acc.count_pair_dims += s1.count_pair_dims;
-        acc.count_skipped_dims += s1.count_skipped_dims;
+        acc.count_fp32_ops += s1.count_fp32_ops;
+        acc.gram_filter |= s1.gram_filter;
         acc.union_pair_dims += s1.union_pair_dims;
         acc.border_pair_dims += s1.border_pair_dims;
         acc.ms_grid += s1.ms_grid;

@@ -626,16 +626,44 @@ __device__ __forceinline__ int row_next(const RowTable &rt, int &row, int t) {
 // of >= min_pts points is all cores (every pair inside it is in range), so its
 // points need no test at all; they report the cell size.
 // ---------------------------------------------------------------------------
-template <int D, bool EARLY>
+//
+// GRAM (d >= 8): a pair is first decided from centred FP32 dot products.  With
+// a = x_i - o and b = x_j - o (o the item's first point), D~ = |a|^2 + |b|^2 - 2 a.b
+// costs d FMAs per pair, against the 3d separately rounded operations of the
+// reference's sum.  A pair is a hit when D~ is below e2 by more than a bound on its
+// error, a miss when above by more than it; the pairs in between (the guard band)
+// are decided by the reference's own FP32 sum.  Counts, lists and core flags are
+// therefore the exact kernel's.  Error bound (u = 2^-24, K = d): centring in FP32
+// moves |a - b|^2 off |x_i - x_j|^2 by at most 4u (n_a + n_b); the FMA chains give
+// |a|^2, |b|^2 and a.b within K u of n_a, n_b and |a||b| <= (n_a + n_b) / 2; forming
+// v = n_a - 2 a.b and v + n_b adds 2u (n_a + n_b).  So |D~ - |x_i - x_j|^2| <=
+// (3K + 6) u (n_a + n_b), and gram_kappa is twice that.  The reference's sum is
+// within (K + 2) u of |x_i - x_j|^2 (gram_gamma covers 2 (K + 8) u), and the
+// thresholds carry the rounding of their own arithmetic (kGramSigma e2).
+// ---------------------------------------------------------------------------
+template <int K>
+__host__ __device__ constexpr float gram_kappa() {
+    return 2.0f * (3.0f * K + 6.0f) * (1.0f / 16777216.0f);
+}
+template <int K>
+__host__ __device__ constexpr float gram_gamma() {
+    return 2.0f * (K + 8) * (1.0f / 16777216.0f);
+}
+constexpr float kGramSigma = 8.0f / 16777216.0f;
+
+template <int D, bool EARLY, bool GRAM = false>
 __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts,
     int dense_skip, int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap,
     int list_stride, unsigned long long *__restrict__ pair_counter, const JobDev *__restrict__ jobs,
     const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev,
-    unsigned long long *__restrict__ skipped_dims) {
+    unsigned long long *__restrict__ band_counter) {
     constexpr int P = Stride<D>::P;
+    static_assert(!GRAM || D >= 8, "the Gram filter is built for d >= 8");
     __shared__ __align__(16) float s_i[kCountWarps][kTile * P];
+    __shared__ __align__(16) float s_a[kCountWarps][GRAM ? kTile * P : 4];  // centred points
+    __shared__ float s_n[kCountWarps][GRAM ? kTile : 1];                     // their squared norms
     __shared__ RowTable s_rows[kCountWarps];
     __shared__ int s_list[kCountWarps][kTile * kSmemListCap];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -663,17 +691,35 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     }
     float *si = s_i[wib];
     RowTable &rt = s_rows[wib];
+    float o[GRAM ? D : 1];  // GRAM: the item's first point, the origin of the centring
+    float nmax = 0.0f;      // GRAM: largest |a|^2 of the item
+    if constexpr (GRAM) load_point<D>(xs, p0, o);
     if (lane < cnt) {
         float x[D];
         load_point<D>(xs, p0 + lane, x);
         store_point_smem<D>(si + lane * P, x);
+        if constexpr (GRAM) {
+            float a[D];
+            float n = 0.0f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                a[k] = __fsub_rn(x[k], o[k]);
+                n = __fmaf_rn(a[k], a[k], n);
+            }
+            store_point_smem<D>(s_a[wib] + lane * P, a);
+            s_n[wib][lane] = n;
+            nmax = n;
+        }
+    }
+    if constexpr (GRAM) {
+#pragma unroll
+        for (int sft = 16; sft > 0; sft >>= 1) nmax = fmaxf(nmax, __shfl_xor_sync(kFull, nmax, sft));
     }
     const int total = gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, rt, lane);
     __syncwarp();
     // running counts in registers: lane k holds the count of the item's point k
     int mycnt = 0;
-    unsigned long long pairs = 0, skipped = 0;  // pairs tested; pairs whose second half was skipped
-    int halves = 0;
+    unsigned long long pairs = 0, band = 0;  // pairs tested; GRAM: pairs rechecked in the guard band
     // points still counting (EARLY: below min_pts), and points whose neighbour list
     // is still filling (count below list_cap): both warp-uniform, updated per chunk
     unsigned act = __ballot_sync(kFull, lane < cnt);
@@ -685,40 +731,63 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     int row = 0;  // this lane's stencil row: its candidate index only grows
     for (int tb = 0; tb < total; tb += kWarp * CH) {
         int j[CH];
-        float xj[CH][D];
+        float xj[CH][D];  // GRAM: the centred candidate b = x_j - o
+        float tlo[CH], thi[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             const int t = tb + c * kWarp + lane;
             j[c] = t < total ? row_next(rt, row, t) : -1;
             if (j[c] >= 0) load_point<D>(xs, j[c], xj[c]);
             else fill_nan<D>(xj[c]);  // NaN fails the predicate
+            if constexpr (GRAM) {
+                float nb = 0.0f;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    xj[c][k] = __fsub_rn(xj[c][k], o[k]);
+                    nb = __fmaf_rn(xj[c][k], xj[c][k], nb);
+                }
+                // hit when v = |a|^2 - 2 a.b <= tlo, miss when v > thi (see the bound above)
+                const float slack = __fadd_rn(__fmul_rn(gram_kappa<D>(), __fadd_rn(nmax, nb)),
+                                              __fmul_rn(kGramSigma, e2));
+                tlo[c] = j[c] >= 0 ? __fsub_rn(__fsub_rn(__fmul_rn(e2, 1.0f - gram_gamma<D>()), nb), slack) : -INFINITY;
+                thi[c] = j[c] >= 0 ? __fadd_rn(__fsub_rn(__fmul_rn(e2, 1.0f + gram_gamma<D>()), nb), slack) : -INFINITY;
+            }
         }
         int active = 0;
         for (unsigned it = act; it; it &= it - 1) {
             const int k = __ffs(it) - 1;
-            float xi[D];
-            load_point_smem<D>(si + k * P, xi);
             bool hit[CH];
             unsigned m[CH];
-            if constexpr (D >= 8) {
-                // the first half of the sum; when no lane's pair can still be in range
-                // the warp skips the second half (exact: the partial sums only grow)
-                constexpr int H = D / 2;
-                float len[CH];
+            if constexpr (GRAM) {
+                float a[D];
+                load_point_smem<D>(s_a[wib] + k * P, a);
+                const float na = s_n[wib][k];
+                bool inband[CH];
 #pragma unroll
-                for (int c = 0; c < CH; ++c) len[c] = dist_part<D, 0, H>(xi, xj[c], 0.0f);
-                bool open = false;
+                for (int c = 0; c < CH; ++c) {
+                    float g = 0.0f;
 #pragma unroll
-                for (int c = 0; c < CH; ++c) open = open || len[c] <= e2;
-                if (__any_sync(kFull, open)) {
+                    for (int q = 0; q < D; ++q) g = __fmaf_rn(a[q], xj[c][q], g);
+                    const float v = __fmaf_rn(-2.0f, g, na);
+                    hit[c] = v <= tlo[c];
+                    inband[c] = !hit[c] && v <= thi[c];
+                }
+                if (inband[0] || (CH > 1 && inband[CH - 1])) {
+                    // the guard band (rare): the reference's own sum decides
+                    float xi[D];
+                    load_point_smem<D>(si + k * P, xi);
 #pragma unroll
-                    for (int c = 0; c < CH; ++c) hit[c] = dist_part<D, H, D>(xi, xj[c], len[c]) <= e2;
-                } else {
-#pragma unroll
-                    for (int c = 0; c < CH; ++c) hit[c] = false;
-                    ++halves;
+                    for (int c = 0; c < CH; ++c) {
+                        if (!inband[c]) continue;
+                        float xr[D];
+                        load_point<D>(xs, j[c], xr);
+                        hit[c] = in_range<D>(xi, xr, e2);
+                        ++band;
+                    }
                 }
             } else {
+                float xi[D];
+                load_point_smem<D>(si + k * P, xi);
 #pragma unroll
                 for (int c = 0; c < CH; ++c) hit[c] = in_range<D>(xi, xj[c], e2);
             }
@@ -745,8 +814,6 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
             ++active;
         }
         pairs += (unsigned long long)active * (unsigned long long)min(kWarp * CH, total - tb);
-        skipped += (unsigned long long)halves * (unsigned long long)min(kWarp * CH, total - tb);
-        halves = 0;
         if (lst) lst &= __ballot_sync(kFull, mycnt < list_cap);
         if (EARLY) {
             act = __ballot_sync(kFull, lane < cnt && mycnt < min_pts);
@@ -765,7 +832,10 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
         }
     }
     if (lane == 0 && pairs) atomicAdd(pair_counter, pairs);
-    if (lane == 0 && skipped) atomicAdd(skipped_dims, skipped * (unsigned long long)(D - D / 2));
+    if constexpr (GRAM) {
+        band = __reduce_add_sync(kFull, (unsigned)band);
+        if (lane == 0 && band) atomicAdd(band_counter, band);
+    }
 }
 
 // Core flags: per sorted point (u8), and a bitmap in input order (one bit per

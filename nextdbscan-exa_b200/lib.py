@@ -119,7 +119,8 @@ class NdbStats(ctypes.Structure):
         ("filter_max_err_over_bound", ctypes.c_double),
         ("filter_audited_pairs", ctypes.c_int64),
         ("filter_misclassified_pairs", ctypes.c_int64),
-        ("count_skipped_dims", ctypes.c_int64),
+        ("count_fp32_ops", ctypes.c_int64),
+        ("gram_filter", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -88,7 +88,16 @@ def run_ranks(world, name, use_gpu=False, full=True):
     procs = [ctx.Process(target=_rank, args=(r, world, port, name, use_gpu, full, q)) for r in range(world)]
     for p in procs:
         p.start()
-    outs = [q.get(timeout=300) for _ in range(world)]
+    import queue
+    import time
+    outs, t0 = [], time.time()
+    while len(outs) < world:  # fail fast when a rank dies instead of waiting out the queue
+        try:
+            outs.append(q.get(timeout=2))
+        except queue.Empty:
+            dead = [p.exitcode for p in procs if p.exitcode not in (None, 0)]
+            assert not dead, f"a rank exited with {dead}"
+            assert time.time() - t0 < 300, "ranks did not report within 300 s"
     for p in procs:
         p.join(120)
         assert p.exitcode == 0
