@@ -733,6 +733,12 @@ void labels_phase(ndb_ctx *ctx) {
     cudaEventRecord(ctx->kev[4], st);  // moved to the main union kernel below when there is one
     if (ctx->n_items > 0) {
         if (ctx->cell_units) {
+            if (ctx->list_cap > 0)
+                ++launch_counter(), union_lists_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+                    nv, ctx->nn_sorted.as<int32_t>(), ctx->nbr_list.as<int32_t>(), ctx->list_cap, ctx->list_cap,
+                    ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(), err, nullptr, nullptr,
+                    ctx->pcell.as<int32_t>(), 1, (ctx->flags_run & NDB_FLAG_FULL_COUNT) == 0,
+                    ctx->cell_start.as<int32_t>(), ctx->min_pts);
             if (ctx->key64)
                 ++launch_counter(), union_near_kernel<D, uint64_t><<<blocks_for(n_cells), kBlock, 0, st>>>(
                     n_cells, ctx->grid, ctx->cell_key.as<uint64_t>(), ctx->cell_start.as<int32_t>(),
@@ -745,19 +751,23 @@ void labels_phase(ndb_ctx *ctx) {
                     cell_index<uint32_t>(ctx), ctx->xs.as<float>(),
                     ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(),
                     ctx->parent.as<int32_t>(), counters + 3, err, nullptr, nullptr);
-            ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
-                                                                                      n_units, err);
+            // comp_min holds the cells' root snapshot until the union is done
+            ++launch_counter(), flatten_snap_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(
+                ctx->parent.as<int32_t>(), n_units, err, ctx->cell_has_core.as<uint8_t>(), ctx->comp_min.as<int32_t>());
             cudaEventRecord(ctx->kev[4], st);
             ++launch_counter(), union_cells_kernel<D><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
                 n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), ctx->n_rows, ctx->xs.as<float>(),
                 ctx->e2, ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
-                counters + 3, err, nullptr, nullptr);
+                counters + 3, err, nullptr, nullptr, ctx->comp_min.as<int32_t>());
+            ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units,
+                                                                                   kNoCluster);
         }
         else {
             if (ctx->list_cap > 0) {
                 ++launch_counter(), union_lists_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
                     nv, ctx->nn_sorted.as<int32_t>(), ctx->nbr_list.as<int32_t>(), ctx->list_cap, ctx->list_cap,
-                    ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(), err, nullptr, nullptr, nullptr);
+                    ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(), err, nullptr, nullptr,
+                    ctx->pcell.as<int32_t>(), 0, 0, ctx->cell_start.as<int32_t>(), ctx->min_pts);
                 ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                           n_units, err);
             }
@@ -1663,21 +1673,29 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     cudaEventRecord(ctx->kev[4], st);
     if (n_items > 0) {
         if (bp.linked) {
+            if (bp.list_stride > 0)
+                ++launch_counter(), union_lists_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
+                    nv, ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, ctx->core_sorted.as<uint8_t>(),
+                    ctx->parent.as<int32_t>(), err, jobs_dev, cell_job, ctx->pcell.as<int32_t>(), 1,
+                    (flags & NDB_FLAG_FULL_COUNT) == 0, ctx->cell_start.as<int32_t>(), 0);
             ++launch_counter(), union_near_kernel<D, K><<<blocks_for(n_cells), kBlock, 0, st>>>(
                 n_cells, bp.jd[0].g, ctx->cell_key.as<K>(), ctx->cell_start.as<int32_t>(), L,
                 ctx->xs.as<float>(), 0.0f, ctx->core_sorted.as<uint8_t>(),
                 ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(), counters + 3, err, jobs_dev, cell_job);
-            ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
-                                                                                      n_units, err);
+            ++launch_counter(), flatten_snap_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(
+                ctx->parent.as<int32_t>(), n_units, err, ctx->cell_has_core.as<uint8_t>(), ctx->comp_min.as<int32_t>());
             ++launch_counter(), union_cells_kernel<D><<<blocks_for(n_cells * kWarp), kBlock, 0, st>>>(
                 n_cells, ctx->cell_start.as<int32_t>(), ctx->nbr.as<int2>(), n_rows, ctx->xs.as<float>(), 0.0f,
                 ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->parent.as<int32_t>(),
-                counters + 3, err, jobs_dev, cell_job);
+                counters + 3, err, jobs_dev, cell_job, ctx->comp_min.as<int32_t>());
+            ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units,
+                                                                                   kNoCluster);
         } else {
             if (bp.list_stride > 0) {
                 ++launch_counter(), union_lists_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
                     nv, ctx->nn_sorted.as<int32_t>(), list, 0, bp.list_stride, ctx->core_sorted.as<uint8_t>(),
-                    ctx->parent.as<int32_t>(), err, jobs_dev, cell_job, ctx->pcell.as<int32_t>());
+                    ctx->parent.as<int32_t>(), err, jobs_dev, cell_job, ctx->pcell.as<int32_t>(), 0, 0,
+                    ctx->cell_start.as<int32_t>(), 0);
                 ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                           n_units, err);
             }

@@ -765,9 +765,12 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
                 bool inband[CH];
 #pragma unroll
                 for (int c = 0; c < CH; ++c) {
-                    float g = 0.0f;
+                    // four independent FMA chains (the bound holds for any order of
+                    // the sum), joined by three additions
+                    float g4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-                    for (int q = 0; q < D; ++q) g = __fmaf_rn(a[q], xj[c][q], g);
+                    for (int q = 0; q < D; ++q) g4[q & 3] = __fmaf_rn(a[q], xj[c][q], g4[q & 3]);
+                    const float g = __fadd_rn(__fadd_rn(g4[0], g4[1]), __fadd_rn(g4[2], g4[3]));
                     const float v = __fmaf_rn(-2.0f, g, na);
                     hit[c] = v <= tlo[c];
                     inband[c] = !hit[c] && v <= thi[c];
@@ -824,9 +827,9 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     if (lane < cnt) nn_sorted[p0 + lane] = mine;
     if (nbr_list && smem_list) {
         __syncwarp();
-        // point units keep every point's list (the union starts from the cores'
-        // lists); cell units only need the lists of the points below min_pts
-        if (lane < cnt && (!dense_skip || mine < min_pts)) {
+        // every point's list: the border step reads the non-cores', the union
+        // starts from the cores' (for cell units, the items the count ran)
+        if (lane < cnt) {
             const int len = min(mine, list_cap);
             for (int q = 0; q < len; ++q) nbr_list[(int64_t)(p0 + lane) * list_stride + q] = sl[lane * kSmemListCap + q];
         }
@@ -1064,12 +1067,16 @@ constexpr int kProbe = 4;  // points of a candidate cell tested by the probe
 //
 // Runs after union_near_kernel has linked the adjacent dense cells, so the root
 // filter removes most candidates before any point test.
+// snap: every cell's root after the near pass (flatten_snap_kernel), -1 for cells
+// without cores; one load per candidate tells both.  A root since hooked elsewhere
+// only costs a needless probe below, never a missed union.
 template <int D>
 __global__ void __launch_bounds__(kBlock) union_cells_kernel(
     int64_t n_cells, const int32_t *__restrict__ cell_start, const int2 *__restrict__ nbr, int n_rows,
     const float *__restrict__ xs, float e2, const uint8_t *__restrict__ core_sorted,
     const uint8_t *__restrict__ cell_has_core, int32_t *parent, unsigned long long *__restrict__ pair_counter,
-    int *err, const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job) {
+    int *err, const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job,
+    const int32_t *__restrict__ snap) {
     constexpr int P = Stride<D>::P;
     __shared__ __align__(16) float s_i[kWarpsPerBlock][kTile * P];
     __shared__ RowTable s_rows[kWarpsPerBlock];
@@ -1084,33 +1091,23 @@ __global__ void __launch_bounds__(kBlock) union_cells_kernel(
     int *sb = s_b[wib];
     const int total = gather_rows<true>(nbr + (int64_t)A * n_rows, n_rows, cell_start, A + 1, rt, lane);
     if (total == 0) return;
-    int rootA = 0;
-    if (lane == 0) rootA = uf_find(parent, A, err);
-    rootA = __shfl_sync(kFull, rootA, 0);
-    // Candidate cells, four per lane per step so that their load chains overlap.  The
-    // root test uses an ancestor two hops up (parents were flattened before this
-    // kernel, so usually the root): equal to A's root means already joined; an
-    // ancestor that is not yet the root only costs a needless probe below.
+    const int rootA = __ldg(snap + A);
+    // Candidate cells, four per lane per step so that their loads overlap: a cell with
+    // cores whose snapshot root differs from A's is a candidate
     constexpr int U = 4;
     int nb = 0;
     for (int tb = 0; tb < total; tb += kWarp * U) {
         int B[U], p[U];
-        bool hc[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int t = tb + u * kWarp + lane;
             B[u] = t < total ? row_lookup(rt, n_rows, t) : -1;
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u) hc[u] = B[u] >= 0 && cell_has_core[B[u]];
-#pragma unroll
-        for (int u = 0; u < U; ++u) p[u] = hc[u] ? __ldcg(parent + B[u]) : -1;
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (hc[u] && p[u] != B[u]) p[u] = __ldcg(parent + p[u]);
+        for (int u = 0; u < U; ++u) p[u] = B[u] >= 0 ? __ldg(snap + B[u]) : -1;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const bool ok = hc[u] && p[u] != rootA;
+            const bool ok = p[u] >= 0 && p[u] != rootA;
             const unsigned mask = __ballot_sync(kFull, ok);
             if (ok) {
                 const int slot = nb + __popc(mask & lanemask_lt());
@@ -1401,25 +1398,37 @@ __global__ void cell_root_kernel(int64_t nv, const int32_t *__restrict__ pcell,
     if (old != -1 && old != r) atomicExch(cell_root + c, -2);
 }
 
-// Point units, first step of the union: every core is joined to the cores among
-// the first neighbours the count recorded for it (at most kListUnions of them; no
-// distance test, each listed point is in range).  Clusters are then nearly all
-// linked, and the candidate scan that follows skips every candidate whose root is
-// already its item's.
+// First step of the union: every core is joined to the cores among the first
+// neighbours the count recorded for it (at most kListUnions of them; no distance
+// test, each listed point is in range).  Point units join the points, cell units
+// their cells.  Clusters are then nearly all linked, and the candidate scans that
+// follow skip every candidate already under the same root.  With the early exit, the
+// count skips the cells of >= min_pts points of a same-cell-linked grid and records no
+// list there (skip_dense): those cells are joined by the near and cell passes.
 constexpr int kListUnions = 8;
 __global__ void union_lists_kernel(int64_t nv, const int32_t *__restrict__ nn_sorted,
                                    const int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
                                    const uint8_t *__restrict__ core_sorted, int32_t *parent, int *err,
                                    const JobDev *__restrict__ jobs, const int32_t *__restrict__ cell_job,
-                                   const int32_t *__restrict__ pcell) {
+                                   const int32_t *__restrict__ pcell, int cell_units, int skip_dense,
+                                   const int32_t *__restrict__ cell_start, int min_pts) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nv || !core_sorted[s]) return;
-    const int cap = jobs ? jobs[cell_job[pcell[s]]].list_cap : list_cap;
+    int cap = list_cap;
+    if (jobs) {
+        const JobDev &J = jobs[cell_job[pcell[s]]];
+        cap = J.list_cap;
+        min_pts = J.min_pts;
+    }
+    const int a = cell_units ? pcell[s] : (int)s;
+    if (cell_units && skip_dense && cell_start[a + 1] - cell_start[a] >= min_pts) return;
     const int len = min(min(nn_sorted[s], cap), kListUnions);
     const int32_t *l = nbr_list + s * list_stride;
     for (int q = 0; q < len; ++q) {
         const int j = l[q];
-        if (j != (int)s && core_sorted[j]) uf_union(parent, (int)s, j, err);
+        if (j == (int)s || !core_sorted[j]) continue;
+        const int b = cell_units ? pcell[j] : j;
+        if (a != b) uf_union(parent, a, b, err);
     }
 }
 
@@ -1430,6 +1439,17 @@ __global__ void flatten_kernel(int32_t *parent, int64_t n_units, int *err) {
     if (u >= n_units) return;
     const int r = uf_find_ro(parent, (int)u, err);
     parent[u] = r;
+}
+
+// The same, also recording each cell's root in snap (-1 for a cell without cores)
+// for the candidate filter of union_cells_kernel.
+__global__ void flatten_snap_kernel(int32_t *parent, int64_t n_units, int *err,
+                                    const uint8_t *__restrict__ has_core, int32_t *__restrict__ snap) {
+    const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n_units) return;
+    const int r = uf_find_ro(parent, (int)u, err);
+    parent[u] = r;
+    snap[u] = has_core[u] ? r : -1;
 }
 
 // ids of the cores in sorted order; counters[0] += component roots (point units)
