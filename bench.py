@@ -480,7 +480,7 @@ def run_ours(args):
         # untimed: the count-kernel thresholds picked on this workload, then left on the context
         r = pkg.autotune.tune_count(ctx, w.coords, w.eps, w.min_pts, full_count=full)
         tuning = {"best": r["best"],
-                  "count_kernel_ms": {f"min_dim={c['tc_min_dim']},min_item={c['tc_min_item']}":
+                  "count_kernel_ms": {f"min_dim={c['tc_min_dim']},min_item={c['tc_min_item']},gram={c['gram_filter']}":
                                       round(c["ms_count_kernel"], 4) for c in r["table"]}}
     clk = ClockSampler(local)
     m = measure_workload(pkg, ctx, w, args.steps, args.warmup, flush, stream, full, ck_kw, not args.no_e2e, world,

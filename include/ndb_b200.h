@@ -76,6 +76,8 @@ typedef enum ndb_status {
                                     * FP32 Gram filter (results are identical either way; this is the plain form) */
 #define NDB_FLAG_TENSOR_FILTER 0x10u /* d >= 8: count on the tensor-core filter whenever the input allows
                                       * it, whatever the tile-fill heuristic would pick (results identical) */
+#define NDB_FLAG_GRAM_FILTER  0x40u  /* d >= 8: the CUDA-core count decides pairs from FP32 Gram dot products
+                                      * first, with a guard band and the exact sum inside it (results identical) */
 #define NDB_FLAG_FILTER_AUDIT 0x20u  /* diagnostic: when the tensor-core filter runs, measure every pair it
                                       * classifies against its FP64 distance and the exact FP32 predicate
                                       * (ndb_stats.filter_*); slower, results identical */
@@ -248,6 +250,8 @@ ndb_status ndb_b200_set_memory_limit(ndb_ctx *ctx, int64_t max_bytes);
 typedef struct ndb_tuning {
     int32_t tc_min_dim;
     int32_t tc_min_item;
+    int32_t gram_filter;  /* 1: the CUDA-core count uses the FP32 Gram filter at d >= 8 (as
+                           * NDB_FLAG_GRAM_FILTER); 0: the library's default (the exact sum) */
 } ndb_tuning;
 
 /* Sets the context's thresholds (NULL: back to the defaults); negative values are

@@ -51,10 +51,11 @@ def _as_points(v_coord, n_dim: int | None = None) -> np.ndarray:
 
 
 def _flags(full_count: bool, approximate: bool, exact_count: bool = False, tensor_filter: bool = False,
-           device: bool = False, audit: bool = False) -> int:
+           device: bool = False, audit: bool = False, gram_filter: bool = False) -> int:
     return ((lib.FLAG_FULL_COUNT if full_count else 0) | (lib.FLAG_APPROXIMATE if approximate else 0)
             | (lib.FLAG_EXACT_COUNT if exact_count else 0) | (lib.FLAG_TENSOR_FILTER if tensor_filter else 0)
-            | (lib.FLAG_DEVICE_PTRS if device else 0) | (lib.FLAG_FILTER_AUDIT if audit else 0))
+            | (lib.FLAG_DEVICE_PTRS if device else 0) | (lib.FLAG_FILTER_AUDIT if audit else 0)
+            | (lib.FLAG_GRAM_FILTER if gram_filter else 0))
 
 
 class Context:
@@ -119,10 +120,10 @@ class Context:
 
     def run(self, coords, eps: float, min_pts: int, *, full_count: bool = False,
             approximate: bool = False, exact_count: bool = False, tensor_filter: bool = False,
-            audit: bool = False) -> tuple[np.ndarray, np.ndarray, Result]:
+            audit: bool = False, gram_filter: bool = False) -> tuple[np.ndarray, np.ndarray, Result]:
         pts = _as_points(coords)
         n, d = pts.shape
-        flags = _flags(full_count, approximate, exact_count, tensor_filter, audit=audit)
+        flags = _flags(full_count, approximate, exact_count, tensor_filter, audit=audit, gram_filter=gram_filter)
         nn = np.empty(n, dtype=np.int32)
         ci = np.empty(n, dtype=np.int32)
         res = lib.NdbResult()
@@ -186,8 +187,8 @@ class Context:
 
     # -- many independent problems in one pipeline ----------------------------
     def run_batched(self, problems, *, full_count: bool = False, approximate: bool = False,
-                    want_nn: bool = True, exact_count: bool = False,
-                    tensor_filter: bool = False) -> list[tuple[np.ndarray | None, np.ndarray, Result]]:
+                    want_nn: bool = True, exact_count: bool = False, tensor_filter: bool = False,
+                    gram_filter: bool = False) -> list[tuple[np.ndarray | None, np.ndarray, Result]]:
         """problems: iterable of (coords n x d, eps, min_pts).  Returns per problem
         (nn, cluster_index, Result), equal to one run() each.  Raises NdbError on
         the first failing problem's status after every other one has run."""
@@ -204,7 +205,7 @@ class Context:
             jobs[j].nn_out = nn.ctypes.data if nn is not None and nn.size else None
             jobs[j].cluster_index_out = ci.ctypes.data if ci.size else None
             outs.append((nn, ci))
-        flags = _flags(full_count, approximate, exact_count, tensor_filter)
+        flags = _flags(full_count, approximate, exact_count, tensor_filter, gram_filter=gram_filter)
         st = self._lib.ndb_b200_run_batched(self._h, jobs, len(pts), flags)
         self.last_jobs = jobs
         lib.check(st, "ndb_b200_run_batched", self._h)
@@ -240,10 +241,10 @@ class Context:
         lib.check(self._lib.ndb_b200_set_memory_limit(self._h, int(max_bytes)), "ndb_b200_set_memory_limit",
                   self._h)
 
-    def set_tuning(self, tc_min_dim: int = 0, tc_min_item: int = 0) -> None:
-        """Count-kernel thresholds of this context (0 = library default); see
+    def set_tuning(self, tc_min_dim: int = 0, tc_min_item: int = 0, gram_filter: int = 0) -> None:
+        """Count-kernel choices of this context (0 = library default); see
         ndb_tuning in include/ndb_b200.h.  Results never depend on them."""
-        t = lib.NdbTuning(int(tc_min_dim), int(tc_min_item))
+        t = lib.NdbTuning(int(tc_min_dim), int(tc_min_item), int(gram_filter))
         lib.check(self._lib.ndb_b200_set_tuning(self._h, ctypes.byref(t)), "ndb_b200_set_tuning", self._h)
 
     def reset_tuning(self) -> None:
@@ -252,7 +253,7 @@ class Context:
     def tuning(self) -> dict:
         t = lib.NdbTuning()
         lib.check(self._lib.ndb_b200_get_tuning(self._h, ctypes.byref(t)), "ndb_b200_get_tuning", self._h)
-        return {"tc_min_dim": t.tc_min_dim, "tc_min_item": t.tc_min_item}
+        return {"tc_min_dim": t.tc_min_dim, "tc_min_item": t.tc_min_item, "gram_filter": t.gram_filter}
 
     def set_debug_limits(self, uf_max_steps: int = 0) -> None:
         """Bound of the device-side union-find loops (0 = the library default); a run

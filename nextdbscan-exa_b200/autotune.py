@@ -1,8 +1,8 @@
 """Autotuner for the neighbour-count thresholds of a context (ndb_tuning).
 
-For d >= 8 the library counts neighbours with the exact FP32 kernel, the
-tensor-core Gram filter, or both, with each item (up to 32 points of one cell)
-sent by its size.  Which is faster depends on the data: how full the items are,
+For d >= 8 the library counts neighbours with the exact FP32 sum, the FP32 Gram
+filter on CUDA cores, the tensor-core Gram filter, or a mix, with each item (up to 32
+points of one cell) sent to the tensor cores by its size.  Which is faster depends on the data: how full the items are,
 d, and whether counts stop early at minPts.  The tuner runs the job under each
 candidate setting and times the count kernels with the library's own device
 events (ndb_stats.ms_count_kernel, min over repetitions).  It requires every
@@ -17,16 +17,20 @@ from __future__ import annotations
 
 import numpy as np
 
-# tc_min_dim above NDB_MAX_DIM keeps every count on the exact kernel
-EXACT_ONLY = {"tc_min_dim": 17, "tc_min_item": 0}
+# tc_min_dim above NDB_MAX_DIM keeps every count on the CUDA cores
+EXACT_ONLY = {"tc_min_dim": 17, "tc_min_item": 0, "gram_filter": 0}
+GRAM_ONLY = {"tc_min_dim": 17, "tc_min_item": 0, "gram_filter": 1}
 ITEM_SIZES = (1, 8, 12, 16, 20, 24, 28, 32)
 
 
 def candidates(d: int) -> list[dict]:
-    """Settings worth timing at dimensionality d (none below the filter's d = 8)."""
+    """Settings worth timing at dimensionality d (none below the filters' d = 8): the
+    exact sum, the FP32 Gram filter, and the tensor-core filter for items of at least
+    k points (the rest on the exact sum)."""
     if d < 8:
         return []
-    return [dict(EXACT_ONLY)] + [{"tc_min_dim": d, "tc_min_item": k} for k in ITEM_SIZES]
+    return [dict(EXACT_ONLY), dict(GRAM_ONLY)] + [{"tc_min_dim": d, "tc_min_item": k, "gram_filter": 0}
+                                                  for k in ITEM_SIZES]
 
 
 def tune_count(ctx, coords, eps: float, min_pts: int, *, full_count: bool = False, reps: int = 3) -> dict:
@@ -59,6 +63,7 @@ def tune_count(ctx, coords, eps: float, min_pts: int, *, full_count: bool = Fals
         ctx.reset_tuning()
         return {"best": None, "table": []}
     best = min(table, key=lambda r: r["ms_count_kernel"])
-    setting = {"tc_min_dim": best["tc_min_dim"], "tc_min_item": best["tc_min_item"]}
+    setting = {"tc_min_dim": best["tc_min_dim"], "tc_min_item": best["tc_min_item"],
+               "gram_filter": best["gram_filter"]}
     ctx.set_tuning(**setting)
     return {"best": setting, "table": table}

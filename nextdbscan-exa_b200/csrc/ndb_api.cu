@@ -74,7 +74,7 @@ struct ndb_ctx {
     // largest device footprint the context may hold (bytes); 0 = no cap
     size_t mem_limit = 0;
     // count-kernel thresholds set by ndb_b200_set_tuning (0: the library's defaults)
-    ndb_tuning tuning{0, 0};
+    ndb_tuning tuning{0, 0, 0};
     // bound of the device-side union-find loops (ndb_b200_set_debug_limits; 0: kUfMaxSteps)
     int uf_max_steps = 0;
 
@@ -149,7 +149,8 @@ struct Fail {
 };
 
 constexpr uint32_t kAllFlags = NDB_FLAG_APPROXIMATE | NDB_FLAG_FULL_COUNT | NDB_FLAG_DEVICE_PTRS |
-                               NDB_FLAG_EXACT_COUNT | NDB_FLAG_TENSOR_FILTER | NDB_FLAG_FILTER_AUDIT;
+                               NDB_FLAG_EXACT_COUNT | NDB_FLAG_TENSOR_FILTER | NDB_FLAG_FILTER_AUDIT |
+                               NDB_FLAG_GRAM_FILTER;
 // internal: the job is the context's loaded copy (ndb_b200_run_loaded); never a caller's flag
 constexpr uint32_t kFlagLoaded = 0x80000000u;
 
@@ -516,11 +517,14 @@ inline bool tc_eligible(const ndb_ctx *ctx, int d, float e2, const double *lo, c
     return true;
 }
 
-// The Gram-filtered count on CUDA cores (count_kernel<D, E, true>): d >= 8, not the
+// The Gram-filtered count on CUDA cores (count_kernel<D, E, true>), when asked for
+// (NDB_FLAG_GRAM_FILTER or the context's tuning; measured on B200 it does not beat
+// the exact sum, whose cost there is latency rather than FP32 issue): d >= 8, not the
 // plain form (NDB_FLAG_EXACT_COUNT), eps^2 a normal float far from under- and
 // overflow, and coordinates within +-2^60 so that no centred square or norm
 // overflows.  Results never depend on it.
-inline bool gram_eligible(int d, float e2, const double *lo, const double *hi, uint32_t flags) {
+inline bool gram_eligible(const ndb_ctx *ctx, int d, float e2, const double *lo, const double *hi, uint32_t flags) {
+    if (!((flags & NDB_FLAG_GRAM_FILTER) || ctx->tuning.gram_filter > 0)) return false;
     if (d < 8 || (flags & NDB_FLAG_EXACT_COUNT)) return false;
     if (!(e2 >= 0x1p-100f && e2 <= 0x1p100f)) return false;
     for (int a = 0; a < d; ++a)
@@ -943,7 +947,7 @@ ndb_status classify_impl(ndb_ctx *ctx, const float *coords, int64_t n, float eps
     ctx->cell_units = pl.cell_units ? 1 : 0;
     if (pl.st.n_rows > kWarp) return NDB_ERR_INVALID_ARGUMENT;  // row tables hold one row per lane
     ctx->tc_count = tc_eligible(ctx, D, ctx->e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
-    ctx->gram_count = gram_eligible(D, ctx->e2, lo, hi, flags);
+    ctx->gram_count = gram_eligible(ctx, D, ctx->e2, lo, hi, flags);
 
     classify_dispatch<D>(ctx, pl);
 
@@ -1307,10 +1311,10 @@ ndb_status ndb_b200_set_memory_limit(ndb_ctx *ctx, int64_t max_bytes) {
 ndb_status ndb_b200_set_tuning(ndb_ctx *ctx, const ndb_tuning *tuning) {
     if (!ctx) return NDB_ERR_INVALID_ARGUMENT;
     if (!tuning) {
-        ctx->tuning = ndb_tuning{0, 0};
+        ctx->tuning = ndb_tuning{0, 0, 0};
         return NDB_OK;
     }
-    if (tuning->tc_min_dim < 0 || tuning->tc_min_item < 0) return NDB_ERR_INVALID_ARGUMENT;
+    if (tuning->tc_min_dim < 0 || tuning->tc_min_item < 0 || tuning->gram_filter < 0) return NDB_ERR_INVALID_ARGUMENT;
     ctx->tuning = *tuning;
     return NDB_OK;
 }
@@ -1897,7 +1901,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
         }
         const Plan pl = plan_grid(D, jd.e2, lo, hi);
         const bool job_tc = tc_eligible(ctx, D, jd.e2, lo, hi, pl.cell_units, pl.st.n_rows, flags);
-        const bool job_gram = gram_eligible(D, jd.e2, lo, hi, flags);
+        const bool job_gram = gram_eligible(ctx, D, jd.e2, lo, hi, flags);
         double cells = 1;
         for (int a = 0; a < pl.g.k; ++a) cells *= (double)pl.g.g[a];
         bool keep = (pl.cell_units ? 1 : 0) == bp.linked && jd.min_pts - 1 <= kMaxListCap &&
@@ -2090,6 +2094,8 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
             stage_batch(ctx, jobs, n_jobs, groups, dj);
         } catch (const Fail &f) {
             cudaStreamSynchronize(ctx->copy_stream);
+            for (int d = 1; d <= NDB_MAX_DIM; ++d)  // every job that was to run carries the failure
+                for (int i : groups[d]) jobs[i].status = f.st;
             return f.st;
         }
         work = dj.data();

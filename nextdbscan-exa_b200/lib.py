@@ -21,6 +21,7 @@ FLAG_DEVICE_PTRS = 0x4
 FLAG_EXACT_COUNT = 0x8
 FLAG_TENSOR_FILTER = 0x10
 FLAG_FILTER_AUDIT = 0x20
+FLAG_GRAM_FILTER = 0x40
 
 STATUS = {
     0: "NDB_OK",
@@ -81,7 +82,7 @@ class NdbJob(ctypes.Structure):
 class NdbTuning(ctypes.Structure):
     """ndb_tuning: count-kernel thresholds of a context (0 = library default)."""
 
-    _fields_ = [("tc_min_dim", ctypes.c_int32), ("tc_min_item", ctypes.c_int32)]
+    _fields_ = [("tc_min_dim", ctypes.c_int32), ("tc_min_item", ctypes.c_int32), ("gram_filter", ctypes.c_int32)]
 
 
 class NdbStats(ctypes.Structure):

@@ -87,5 +87,5 @@ def test_autotune_candidates():
     at = load_pkg().autotune
     assert at.candidates(3) == []
     c8 = at.candidates(8)
-    assert c8[0] == at.EXACT_ONLY and len(c8) == 1 + len(at.ITEM_SIZES)
-    assert all(c["tc_min_dim"] == 8 for c in c8[1:])
+    assert c8[0] == at.EXACT_ONLY and c8[1] == at.GRAM_ONLY and len(c8) == 2 + len(at.ITEM_SIZES)
+    assert all(c["tc_min_dim"] == 8 for c in c8[2:])

@@ -1,7 +1,7 @@
 """The FP32 Gram-filtered count on CUDA cores (d >= 8): centred dot products decide
 a pair outside a guard band that bounds their error, and the reference's own FP32
-sum decides the pairs inside it.  It is the library's default CUDA-core count for
-d >= 8; the plain form (NDB_FLAG_EXACT_COUNT) never uses it.  Counts, core flags,
+sum decides the pairs inside it.  It runs when asked for (NDB_FLAG_GRAM_FILTER, or a
+context's tuning); the plain form (NDB_FLAG_EXACT_COUNT) never uses it.  Counts, core flags,
 cluster ids and meta must be bit-identical to the exact kernel's and the oracle's,
 including pairs exactly at eps, coordinates far from the origin, tiny eps, and
 special values."""
@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 
 def both(ctx, x, eps, m, full=True):
-    nn_g, ci_g, r_g = ctx.run(x, eps, m, full_count=full)
+    nn_g, ci_g, r_g = ctx.run(x, eps, m, full_count=full, gram_filter=True)
     s_g = ctx.stats()
     nn_e, ci_e, r_e = ctx.run(x, eps, m, full_count=full, exact_count=True)
     s_e = ctx.stats()
@@ -51,7 +51,7 @@ def test_gram_equals_exact_kernel(ctx, d, full):
 def test_gram_against_oracle_8d(ctx, pkg):
     w = pkg.synthetic.config3(n=60_000)
     nn_o, ci_o, meta = oracle.cells(w.coords, w.eps, w.min_pts)
-    nn, ci, res = ctx.run(w.coords, w.eps, w.min_pts, full_count=True)
+    nn, ci, res = ctx.run(w.coords, w.eps, w.min_pts, full_count=True, gram_filter=True)
     assert ctx.stats()["gram_filter"] == 1
     np.testing.assert_array_equal(nn, nn_o)
     np.testing.assert_array_equal(ci, ci_o)
@@ -99,9 +99,23 @@ def test_gram_with_special_values(ctx):
 
 def test_gram_in_batches(ctx, pkg):
     jobs = pkg.synthetic.config4(n_jobs=40, seed=31, n_min=500, n_max=9000, dims=(8, 16))
-    outs = ctx.run_batched([(j.coords, j.eps, j.min_pts) for j in jobs], full_count=True)
+    outs = ctx.run_batched([(j.coords, j.eps, j.min_pts) for j in jobs], full_count=True, gram_filter=True)
     assert ctx.stats()["gram_filter"] == 1
     for j, (nn, ci, res) in zip(jobs, outs):
         nn_e, ci_e, r_e = ctx.run(j.coords, j.eps, j.min_pts, full_count=True, exact_count=True)
         np.testing.assert_array_equal(nn, nn_e)
         np.testing.assert_array_equal(ci, ci_e)
+
+
+def test_gram_through_the_tuning(ctx):
+    rng = np.random.default_rng(8)
+    x = rng.normal(0, 1, (6000, 10)).astype(np.float32)
+    ctx.set_tuning(tc_min_dim=17, gram_filter=1)
+    try:
+        nn, ci, _ = ctx.run(x, 1.9, 6, full_count=True)
+        assert ctx.stats()["gram_filter"] == 1
+    finally:
+        ctx.reset_tuning()
+    nn_e, ci_e, _ = ctx.run(x, 1.9, 6, full_count=True, exact_count=True)
+    np.testing.assert_array_equal(nn, nn_e)
+    np.testing.assert_array_equal(ci, ci_e)

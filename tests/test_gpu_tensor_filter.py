@@ -130,9 +130,9 @@ def test_tuning_and_autotuner(ctx, pkg):
         r = pkg.autotune.tune_count(ctx, w.coords, w.eps, w.min_pts, full_count=True, reps=2)
         assert r["best"] in pkg.autotune.candidates(8)
         assert ctx.tuning() == r["best"]
-        by = {(t["tc_min_dim"], t["tc_min_item"]): t for t in r["table"]}
-        assert by[(17, 0)]["tensor_items"] == 0
-        assert by[(8, 1)]["tensor_items"] > 0
+        by = {(t["tc_min_dim"], t["tc_min_item"], t["gram_filter"]): t for t in r["table"]}
+        assert by[(17, 0, 0)]["tensor_items"] == 0 and by[(17, 0, 1)]["tensor_items"] == 0
+        assert by[(8, 1, 0)]["tensor_items"] > 0
         nn, ci, _ = ctx.run(w.coords, w.eps, w.min_pts, full_count=True)
         np.testing.assert_array_equal(nn, nn_o)
         np.testing.assert_array_equal(ci, ci_o)
@@ -150,7 +150,7 @@ def test_tuning_and_autotuner(ctx, pkg):
             ctx.set_tuning(tc_min_dim=-1)
     finally:
         ctx.reset_tuning()
-    assert ctx.tuning() == {"tc_min_dim": 0, "tc_min_item": 0}
+    assert ctx.tuning() == {"tc_min_dim": 0, "tc_min_item": 0, "gram_filter": 0}
 
 
 @pytest.mark.parametrize("full", [True, False])
