@@ -187,6 +187,8 @@ def cpu_reference(pkg, config: int, sample_n: int, threads: int, steps: int = 1,
     oracle = _ensure_ref()
     import inspect
     full_n = inspect.signature(getattr(pkg.synthetic, f"config{config}")).parameters["n"].default
+    if full_n <= 100_000:  # the 2-D 100k workload is timed whole: a few seconds of reference work
+        sample_n = full_n
     w = pkg.synthetic.make(config, n=min(sample_n, full_n))
     if oracle.have_ref():
         kind = "reference"
