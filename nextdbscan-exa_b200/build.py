@@ -74,7 +74,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
                 f.result()
     if jobs or not os.path.exists(LIB):
         cmd = [nvcc_path(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs,
-               "-lcudart"]
+               "-lcudart", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

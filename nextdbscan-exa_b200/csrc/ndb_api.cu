@@ -6,8 +6,13 @@
 #include <string.h>
 
 #include <algorithm>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ndb_b200.h"
@@ -60,8 +65,15 @@ struct ndb_ctx {
     DevBuf ids_in;
     // batched runs on host buffers: every job's coordinates and outputs on the device
     DevBuf batch_in, batch_nn, batch_ci;
-    cudaEvent_t ev_grp[NDB_MAX_DIM + 1] = {};  // a group's inputs are on the device
-    cudaEvent_t ev_out = nullptr;              // a group's outputs are ready
+    cudaEvent_t ev_grp[NDB_MAX_DIM + 1] = {};   // a group's inputs are on the device
+    cudaEvent_t ev_done[NDB_MAX_DIM + 2] = {};  // a group's outputs are ready (last: the solo jobs')
+    // batched runs: the pipelines' small host <-> device transfers (job tables,
+    // bounding boxes, sizes, counters) go through this mapped pinned buffer with copy
+    // kernels, so they never queue behind the copy engines' transfers of the other
+    // groups' inputs and outputs
+    char *mail = nullptr;      // host address; the device reads and writes it (mapped)
+    char *mail_dev = nullptr;  // its device address
+    size_t mail_bytes = 0, mail_used = 0;
     // ndb_b200_load_bin: two pinned staging chunks, the loaded job (its coordinates in
     // `coords`) and its bounding box, reduced chunk by chunk while it arrived
     void *pin[2] = {nullptr, nullptr};
@@ -188,6 +200,77 @@ T *small_at(ndb_ctx *ctx, size_t off) {
 inline cudaEvent_t lazy_event(ndb_ctx *ctx, cudaEvent_t &e) {
     if (!e) ck(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return e;
+}
+
+// Sets `bytes` bytes at p to v with a kernel (a memset that never waits for a copy
+// engine).
+inline void fill_bytes(ndb_ctx *ctx, void *p, int v, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return;
+    const int64_t n16 = ((uintptr_t)p & 15) ? 0 : (int64_t)(bytes / 16);
+    const unsigned blocks = (unsigned)std::min<int64_t>(std::max<int64_t>((n16 + kBlock - 1) / kBlock, 1),
+                                                        int64_t(ctx->sm_count) * 8);
+    ++launch_counter(), fill_bytes_kernel<<<blocks, kBlock, 0, st>>>(static_cast<uint8_t *>(p), bytes, n16,
+                                                                   (uint8_t)v);
+    ck(ctx, cudaGetLastError());
+}
+
+// The mailbox holds at least `bytes`; grown only between runs (nothing of the
+// context in flight).
+inline void ensure_mail(ndb_ctx *ctx, size_t bytes) {
+    if (bytes <= ctx->mail_bytes) return;
+    bytes = (bytes + (size_t(1) << 20) - 1) & ~((size_t(1) << 20) - 1);
+    if (ctx->mail) {
+        cudaFreeHost(ctx->mail);
+        ctx->mail = ctx->mail_dev = nullptr;
+        ctx->mail_bytes = 0;
+    }
+    void *h = nullptr, *d = nullptr;
+    ck(ctx, cudaHostAlloc(&h, bytes, cudaHostAllocMapped));
+    if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+        cudaFreeHost(h);
+        ck(ctx, cudaErrorInvalidValue);
+    }
+    ctx->mail = static_cast<char *>(h);
+    ctx->mail_dev = static_cast<char *>(d);
+    ctx->mail_bytes = bytes;
+}
+
+// A 16-byte aligned slice of the mailbox; slices are handed out in order and
+// released together (mail_used = 0) once the stream has drained.
+inline char *mail_slice(ndb_ctx *ctx, size_t bytes) {
+    const size_t off = (ctx->mail_used + 15) & ~size_t(15);
+    if (!ctx->mail || off + bytes > ctx->mail_bytes) ck(ctx, cudaErrorInvalidValue);
+    ctx->mail_used = off + bytes;
+    return ctx->mail + off;
+}
+
+inline void copy_words(ndb_ctx *ctx, const void *src, void *dst, size_t bytes, cudaStream_t st) {
+    const int64_t n = (int64_t)(bytes / 4);
+    if (n == 0) return;
+    const unsigned blocks = (unsigned)std::min<int64_t>((n + kBlock - 1) / kBlock, int64_t(ctx->sm_count) * 4);
+    ++launch_counter(), copy_words_kernel<<<blocks, kBlock, 0, st>>>(static_cast<const uint32_t *>(src),
+                                                                   static_cast<uint32_t *>(dst), n);
+    ck(ctx, cudaGetLastError());
+}
+
+// Device -> host through the mailbox: a copy kernel in stream order; the returned
+// host copy is valid once the stream is synchronized.
+template <typename T>
+const T *mail_from_device(ndb_ctx *ctx, const T *src, size_t count, cudaStream_t st) {
+    static_assert(sizeof(T) % 4 == 0, "mailbox transfers are whole words");
+    char *h = mail_slice(ctx, count * sizeof(T));
+    copy_words(ctx, src, ctx->mail_dev + (h - ctx->mail), count * sizeof(T), st);
+    return reinterpret_cast<const T *>(h);
+}
+
+// Host -> device through the mailbox: the data is copied into the mailbox now and
+// moved by a copy kernel in stream order.
+template <typename T>
+void mail_to_device(ndb_ctx *ctx, T *dst, const T *src, size_t count, cudaStream_t st) {
+    static_assert(sizeof(T) % 4 == 0, "mailbox transfers are whole words");
+    char *h = mail_slice(ctx, count * sizeof(T));
+    memcpy(h, src, count * sizeof(T));
+    copy_words(ctx, ctx->mail_dev + (h - ctx->mail), dst, count * sizeof(T), st);
 }
 
 // ---------------------------------------------------------------------------
@@ -360,7 +443,7 @@ CellIndex<K> build_cell_index(ndb_ctx *ctx, int64_t n_cells, double columns, con
     if (ctx->use_cols) {
         const size_t cols = (size_t)columns;
         ensure(ctx, ctx->col_range, (cols + 1) * sizeof(int2));
-        ck(ctx, cudaMemsetAsync(ctx->col_range.ptr, 0, (cols + 1) * sizeof(int2), st));
+        fill_bytes(ctx, ctx->col_range.ptr, 0, (size_t)(cols + 1) * sizeof(int2), st);
         ++launch_counter(), col_range_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
             ctx->cell_key.as<K>(), n_cells, g_one, jobs, cell_job, ctx->col_range.as<int2>());
         ck(ctx, cudaGetLastError());
@@ -561,7 +644,7 @@ void launch_count_tc(ndb_ctx *ctx, int64_t n_items, const int2 *items, const int
         cudaStream_t st = ctx->stream;
         unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
         unsigned int *work = reinterpret_cast<unsigned int *>(counters + 6);
-        ck(ctx, cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
+        fill_bytes(ctx, work, 0, sizeof(unsigned long long), st);
         const unsigned grid = (unsigned)std::min<int64_t>(n_items, (int64_t)ctx->sm_count * 4);
         if (audit)
             ++launch_counter(), tc::count_tc_kernel<D, true><<<grid, tc::kThreads, 0, st>>>(
@@ -597,7 +680,7 @@ void count_items(ndb_ctx *ctx, bool tc, bool force_tc, bool gram, bool early, in
         ensure(ctx, ctx->items_split, (size_t)(2 * n_items + 2) * sizeof(int2));
         int2 *tc_items = ctx->items_split.as<int2>();
         int2 *rest = tc_items + n_items + 1;
-        ck(ctx, cudaMemsetAsync(scal + 4, 0, 2 * sizeof(uint32_t), st));
+        fill_bytes(ctx, scal + 4, 0, 2 * sizeof(uint32_t), st);
         ++launch_counter(), split_items_kernel<<<blocks_for(n_items), kBlock, 0, st>>>(
             items, n_items, cell_start, force_tc ? 1 : ctx_tc_min_item(ctx), tc_items, scal + 4, rest, scal + 5);
         ck(ctx, cudaGetLastError());
@@ -661,8 +744,8 @@ void core_flags_phase(ndb_ctx *ctx) {
     ensure(ctx, ctx->cell_has_core, ctx->n_cells + 1);
     ensure(ctx, ctx->core_bits, (n_words + 1) * sizeof(uint32_t));
     ensure(ctx, ctx->core_prefix, (n_words + 1) * sizeof(uint32_t));
-    ck(ctx, cudaMemsetAsync(ctx->cell_has_core.ptr, 0, ctx->n_cells + 1, st));
-    ck(ctx, cudaMemsetAsync(ctx->core_bits.ptr, 0, (n_words + 1) * sizeof(uint32_t), st));
+    fill_bytes(ctx, ctx->cell_has_core.ptr, 0, (size_t)ctx->n_cells + 1, st);
+    fill_bytes(ctx, ctx->core_bits.ptr, 0, (size_t)(n_words + 1) * sizeof(uint32_t), st);
     ++launch_counter(), core_flags_kernel<<<blocks_for(n), kBlock, 0, st>>>(
         ctx->nn_sorted.as<int32_t>(), ctx->nv, n, ctx->min_pts, ctx->ids0.as<int32_t>(), ctx->pcell.as<int32_t>(),
         ctx->core_sorted.as<uint8_t>(), ctx->cell_has_core.as<uint8_t>(), ctx->core_bits.as<uint32_t>(), nullptr,
@@ -775,7 +858,7 @@ void labels_phase(ndb_ctx *ctx) {
                 ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                           n_units, err);
             }
-            ck(ctx, cudaMemsetAsync(ctx->cell_cid.ptr, 0xff, (size_t)n_cells * sizeof(int32_t), st));  // -1
+            fill_bytes(ctx, ctx->cell_cid.ptr, 0xff, (size_t)n_cells * sizeof(int32_t), st);  // -1
             ++launch_counter(), cell_root_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
                 nv, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(),
                 ctx->cell_cid.as<int32_t>());
@@ -1283,11 +1366,13 @@ ndb_status ndb_b200_destroy(ndb_ctx *ctx) {
     if (ctx->ev_nn) cudaEventDestroy(ctx->ev_nn);
     for (auto &e : ctx->ev_grp)
         if (e) cudaEventDestroy(e);
-    if (ctx->ev_out) cudaEventDestroy(ctx->ev_out);
+    for (auto &e : ctx->ev_done)
+        if (e) cudaEventDestroy(e);
     for (int b = 0; b < 2; ++b) {
         if (ctx->ev_pin[b]) cudaEventDestroy(ctx->ev_pin[b]);
         if (ctx->pin[b]) cudaFreeHost(ctx->pin[b]);
     }
+    if (ctx->mail) cudaFreeHost(ctx->mail);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -1594,10 +1679,9 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     ++launch_counter(), gather_kernel<D><<<blocks_for(nv), kBlock, 0, st>>>(ctx->coords.as<float>(), perm, nv,
                                                                            ctx->xs.as<float>());
     ck(ctx, cudaGetLastError());
-    uint32_t n_cells32 = 0;
-    ck(ctx, cudaMemcpyAsync(&n_cells32, scal + 0, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    const uint32_t *m_cells = mail_from_device(ctx, scal + 0, 1, st);
     ck(ctx, cudaStreamSynchronize(st));
-    const int64_t n_cells = nv > 0 ? n_cells32 : 0;
+    const int64_t n_cells = nv > 0 ? *m_cells : 0;
     ensure(ctx, ctx->cell_job, (n_cells + 1) * sizeof(int32_t));
     ++launch_counter(), cell_job_kernel<K><<<blocks_for(n_cells), kBlock, 0, st>>>(
         ctx->cell_key.as<K>(), n_cells, jobs_dev, nj, ctx->cell_job.as<int32_t>());
@@ -1608,7 +1692,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     const CellIndex<K> L = build_cell_index<K>(ctx, n_cells, (double)bp.columns, bp.jd[0].g, jobs_dev, cell_job);
     ensure(ctx, ctx->nbr, (size_t)(n_cells * n_rows + 1) * sizeof(int2));
     int4 *rows_dev = small_at<int4>(ctx, kSmallStencilOff);
-    ck(ctx, cudaMemcpyAsync(rows_dev, bp.st.rows, n_rows * sizeof(int4), cudaMemcpyHostToDevice, st));
+    mail_to_device(ctx, rows_dev, bp.st.rows, (size_t)n_rows, st);
     const int rlog = row_group_log2(n_rows);
     ++launch_counter(), rows_kernel<K><<<blocks_for(n_cells << rlog), kBlock, 0, st>>>(
         ctx->cell_key.as<K>(), n_cells, bp.jd[0].g, rows_dev, n_rows, rlog, L, ctx->nbr.as<int2>(), jobs_dev,
@@ -1621,10 +1705,9 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         ctx->cell_start.as<int32_t>(), n_cells, ctx->item_cnt.as<uint32_t>());
     ck(ctx, scan_exclusive_u32(ctx->item_cnt.as<uint32_t>(), ctx->item_cnt.as<uint32_t>(), n_cells, scal + 1,
                                ctx->scan_scratch.as<uint32_t>(), st));
-    uint32_t n_items32 = 0;
-    ck(ctx, cudaMemcpyAsync(&n_items32, scal + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    const uint32_t *m_items = mail_from_device(ctx, scal + 1, 1, st);
     ck(ctx, cudaStreamSynchronize(st));
-    const int64_t n_items = n_cells > 0 ? n_items32 : 0;
+    const int64_t n_items = n_cells > 0 ? *m_items : 0;
     ensure(ctx, ctx->items, (n_items + 1) * sizeof(int2));
     ++launch_counter(), item_write_kernel<<<blocks_for(n_cells), kBlock, 0, st>>>(
         ctx->cell_start.as<int32_t>(), n_cells, ctx->item_cnt.as<uint32_t>(), ctx->items.as<int2>());
@@ -1650,8 +1733,8 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     ensure(ctx, ctx->cell_has_core, n_cells + 1);
     ensure(ctx, ctx->core_bits, (n_words + 1) * sizeof(uint32_t));
     ensure(ctx, ctx->core_prefix, (n_words + 1) * sizeof(uint32_t));
-    ck(ctx, cudaMemsetAsync(ctx->cell_has_core.ptr, 0, n_cells + 1, st));
-    ck(ctx, cudaMemsetAsync(ctx->core_bits.ptr, 0, (n_words + 1) * sizeof(uint32_t), st));
+    fill_bytes(ctx, ctx->cell_has_core.ptr, 0, (size_t)n_cells + 1, st);
+    fill_bytes(ctx, ctx->core_bits.ptr, 0, (size_t)(n_words + 1) * sizeof(uint32_t), st);
     ++launch_counter(), core_flags_kernel<<<blocks_for(n), kBlock, 0, st>>>(
         ctx->nn_sorted.as<int32_t>(), nv, n, 0, perm, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(),
         ctx->cell_has_core.as<uint8_t>(), ctx->core_bits.as<uint32_t>(), jobs_dev, cell_job, nj);
@@ -1670,7 +1753,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
     ensure(ctx, ctx->cell_cid, (n_cells + 1) * sizeof(int32_t));
     ensure(ctx, ctx->job_counters, (size_t)(4 * nj + 4) * sizeof(unsigned long long));
     unsigned long long *jc = ctx->job_counters.as<unsigned long long>();
-    ck(ctx, cudaMemsetAsync(jc, 0, (size_t)(4 * nj + 4) * sizeof(unsigned long long), st));
+    fill_bytes(ctx, jc, 0, (size_t)(4 * nj + 4) * sizeof(unsigned long long), st);
     ++launch_counter(), iota_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(), n_units);
     ++launch_counter(), fill_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->comp_min.as<int32_t>(), n_units,
                                                                            kNoCluster);
@@ -1703,7 +1786,7 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
                 ++launch_counter(), flatten_kernel<<<blocks_for(n_units), kBlock, 0, st>>>(ctx->parent.as<int32_t>(),
                                                                                           n_units, err);
             }
-            ck(ctx, cudaMemsetAsync(ctx->cell_cid.ptr, 0xff, (size_t)n_cells * sizeof(int32_t), st));  // -1
+            fill_bytes(ctx, ctx->cell_cid.ptr, 0xff, (size_t)n_cells * sizeof(int32_t), st);  // -1
             ++launch_counter(), cell_root_kernel<<<blocks_for(nv), kBlock, 0, st>>>(
                 nv, ctx->pcell.as<int32_t>(), ctx->core_sorted.as<uint8_t>(), ctx->parent.as<int32_t>(),
                 ctx->cell_cid.as<int32_t>());
@@ -1753,18 +1836,13 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         jobs_dev, nj, ctx->core_bits.as<uint32_t>(), ctx->core_prefix.as<uint32_t>(), n, jc);
     ck(ctx, cudaGetLastError());
     cudaEventRecord(ctx->ev[4], st);
-    std::vector<unsigned long long> h_jc((size_t)4 * nj);
-    unsigned long long h_pairs[4] = {0, 0, 0, 0};  // count, union, border, band pairs (running totals)
-    unsigned long long h_audit[4] = {0, 0, 0, 0};  // filter audit (running over the call's pipelines)
-    uint32_t h_tc_items = 0;
-    int h_err = 0;
-    if (bp.tc)
-        ck(ctx, cudaMemcpyAsync(&h_tc_items, scal + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    ck(ctx, cudaMemcpyAsync(h_pairs, counters + 2, sizeof(h_pairs), cudaMemcpyDeviceToHost, st));
-    ck(ctx, cudaMemcpyAsync(h_audit, counters + 8, sizeof(h_audit), cudaMemcpyDeviceToHost, st));
-    ck(ctx, cudaMemcpyAsync(h_jc.data(), jc, (size_t)4 * nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                            st));
-    ck(ctx, cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // count, union, border, band pairs (running totals), then the filter audit
+    // (running over the call's pipelines)
+    const unsigned long long *m_pairs = mail_from_device(ctx, counters + 2, 4, st);
+    const unsigned long long *m_audit = mail_from_device(ctx, counters + 8, 4, st);
+    const unsigned long long *m_jc = mail_from_device(ctx, jc, (size_t)4 * nj, st);
+    const uint32_t *m_tc = mail_from_device(ctx, scal + 4, 1, st);
+    const int *m_err = mail_from_device(ctx, err, 1, st);
     if (!(flags & NDB_FLAG_DEVICE_PTRS)) {
         for (int m = 0; m < nj; ++m) {
             ndb_job &J = jobs[members[m]];
@@ -1778,6 +1856,12 @@ void run_group_keys(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members
         }
     }
     ck(ctx, cudaStreamSynchronize(st));
+    unsigned long long h_pairs[4], h_audit[4];
+    memcpy(h_pairs, m_pairs, sizeof(h_pairs));
+    memcpy(h_audit, m_audit, sizeof(h_audit));
+    const std::vector<unsigned long long> h_jc(m_jc, m_jc + (size_t)4 * nj);
+    const uint32_t h_tc_items = bp.tc ? *m_tc : 0;
+    const int h_err = *m_err;
     // statistics summed over the pipelines of one batched call
     ndb_stats &S = ctx->stats;
     S.pipelines += 1;
@@ -1832,6 +1916,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
                std::vector<int> &solo) {
     if (members.empty()) return;
     cudaStream_t st = ctx->stream;
+    ctx->mail_used = 0;  // the stream has drained: every earlier mailbox slice is consumed
     const int nj = (int)members.size();
     BatchPlan bp;
     bp.jd.resize(nj);
@@ -1852,7 +1937,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
     const int64_t n = off;
     ensure(ctx, ctx->coords, (size_t)n * D * sizeof(float));
     ensure(ctx, ctx->jobs_dev, (size_t)nj * sizeof(JobDev));
-    ck(ctx, cudaMemcpyAsync(ctx->jobs_dev.ptr, bp.jd.data(), (size_t)nj * sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    mail_to_device(ctx, ctx->jobs_dev.as<JobDev>(), bp.jd.data(), (size_t)nj, st);
     const unsigned gx = (unsigned)std::min<int64_t>((max_n + kBlock - 1) / kBlock, 64);
     if (flags & NDB_FLAG_DEVICE_PTRS) {
         ++launch_counter(), gather_jobs_kernel<D><<<dim3(gx, nj), kBlock, 0, st>>>(ctx->jobs_dev.as<JobDev>(),
@@ -1874,11 +1959,11 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
     ++launch_counter(), bbox_batch_kernel<D><<<dim3(gx, nj), kBlock, 0, st>>>(ctx->coords.as<float>(),
                                                                              ctx->jobs_dev.as<JobDev>(), lo_hi, inval);
     ck(ctx, cudaGetLastError());
-    std::vector<int> h_lo_hi((size_t)nj * 2 * D);
-    std::vector<unsigned long long> h_inval(nj);
-    ck(ctx, cudaMemcpyAsync(h_lo_hi.data(), lo_hi, h_lo_hi.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
-    ck(ctx, cudaMemcpyAsync(h_inval.data(), inval, nj * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    const int *m_lo_hi = mail_from_device(ctx, lo_hi, (size_t)nj * 2 * D, st);
+    const unsigned long long *m_inval = mail_from_device(ctx, inval, (size_t)nj, st);
     ck(ctx, cudaStreamSynchronize(st));
+    const std::vector<int> h_lo_hi(m_lo_hi, m_lo_hi + (size_t)nj * 2 * D);
+    const std::vector<unsigned long long> h_inval(m_inval, m_inval + nj);
 
     auto dec = [](int v) {
         const int i = v >= 0 ? v : v ^ 0x7fffffff;
@@ -1976,7 +2061,7 @@ void run_group(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &members, uin
             bp.jd[m].ci_out = jobs[members[m]].cluster_index_out ? ctx->ci_orig.as<int32_t>() + bp.jd[m].off : nullptr;
         }
     }
-    ck(ctx, cudaMemcpyAsync(ctx->jobs_dev.ptr, bp.jd.data(), (size_t)nj * sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    mail_to_device(ctx, ctx->jobs_dev.as<JobDev>(), bp.jd.data(), (size_t)nj, st);
     if (bits <= 32) run_group_keys<D, uint32_t>(ctx, jobs, members, bp, flags);
     else run_group_keys<D, uint64_t>(ctx, jobs, members, bp, flags);
 }
@@ -1994,12 +2079,12 @@ ndb_status run_group_entry(ndb_ctx *ctx, ndb_job *jobs, const std::vector<int> &
     }
 }
 
-// Host buffers of a batched run: every job's coordinates go to the device on the
-// copy stream, group after group in the order the groups run, with an event per
-// group; the jobs the pipelines see (dj) point at the device copies and at device
-// output slots.  Later groups' copies then overlap earlier groups' compute.
-void stage_batch(ndb_ctx *ctx, const ndb_job *jobs, int64_t n_jobs, const std::vector<std::vector<int>> &groups,
-                 std::vector<ndb_job> &dj) {
+// Host buffers of a batched run: the device copies of every job's coordinates and
+// output slots, group after group in the order the groups run; the jobs the
+// pipelines see (dj) point at them.  Allocation happens here, on the calling
+// thread, before any copy is issued.
+void plan_stage(ndb_ctx *ctx, const ndb_job *jobs, int64_t n_jobs, const std::vector<std::vector<int>> &groups,
+                std::vector<ndb_job> &dj) {
     size_t nf = 0, np = 0;
     bool want_nn = false, want_ci = false;
     for (int d = 1; d <= NDB_MAX_DIM; ++d)
@@ -2018,34 +2103,123 @@ void stage_batch(ndb_ctx *ctx, const ndb_job *jobs, int64_t n_jobs, const std::v
         if (groups[d].empty()) continue;
         for (int i : groups[d]) {
             const ndb_job &J = jobs[i];
-            float *dst = ctx->batch_in.as<float>() + f;
-            ck(ctx, cudaMemcpyAsync(dst, J.coords, (size_t)J.n * d * sizeof(float), cudaMemcpyHostToDevice,
-                                    ctx->copy_stream));
-            dj[i].coords = dst;
+            dj[i].coords = ctx->batch_in.as<float>() + f;
             dj[i].nn_out = J.nn_out ? ctx->batch_nn.as<int32_t>() + p : nullptr;
             dj[i].cluster_index_out = J.cluster_index_out ? ctx->batch_ci.as<int32_t>() + p : nullptr;
             f += (size_t)J.n * d;
             p += (size_t)J.n;
         }
-        ck(ctx, cudaEventRecord(lazy_event(ctx, ctx->ev_grp[d]), ctx->copy_stream));
+        lazy_event(ctx, ctx->ev_grp[d]);
+        lazy_event(ctx, ctx->ev_done[d]);
     }
+    lazy_event(ctx, ctx->ev_done[NDB_MAX_DIM + 1]);
 }
 
-// Outputs of finished jobs back to the caller's buffers on the copy stream, after
-// the work queued so far on the context's stream: they overlap what comes next.
-void unstage_jobs(ndb_ctx *ctx, const ndb_job *jobs, const std::vector<ndb_job> &dj, const std::vector<int> &which) {
-    if (which.empty()) return;
-    ck(ctx, cudaEventRecord(lazy_event(ctx, ctx->ev_out), ctx->stream));
-    ck(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_out, 0));
-    for (int i : which) {
+// Issues a batched call's host copies from a second host thread, in order, on the
+// copy stream.  A batch of thousands of jobs needs thousands of copy calls; issued
+// there they run while the calling thread drives the pipelines, so the device does
+// not idle between groups while the host queues one group's output copies or the
+// next groups' input copies.  Marks let the calling thread wait until a group's
+// input copies (and the event after them) are queued.
+class CopyIssuer {
+  public:
+    explicit CopyIssuer(int device) : device_(device), th_([this] { loop(); }) {}
+    ~CopyIssuer() { finish(); }
+    void push(std::function<cudaError_t()> task) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            tasks_.push_back(std::move(task));
+        }
+        cv_.notify_all();
+    }
+    // a task that records mark m as reached
+    void mark(int m) {
+        push([this, m] {
+            std::lock_guard<std::mutex> lk(mu_);
+            marks_.push_back(m);
+            cv_.notify_all();
+            return cudaSuccess;
+        });
+    }
+    // blocks until mark m is reached (true) or a task failed (false)
+    bool wait_mark(int m) {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] {
+            return err_ != cudaSuccess || std::find(marks_.begin(), marks_.end(), m) != marks_.end();
+        });
+        return err_ == cudaSuccess;
+    }
+    // runs the remaining tasks and joins; the first failure
+    cudaError_t finish() {
+        if (th_.joinable()) {
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                done_ = true;
+            }
+            cv_.notify_all();
+            th_.join();
+        }
+        return err_;
+    }
+
+  private:
+    void loop() {
+        cudaError_t e = cudaSetDevice(device_);
+        for (;;) {
+            std::function<cudaError_t()> task;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                if (e != cudaSuccess && err_ == cudaSuccess) {
+                    err_ = e;  // later tasks are dropped; waiters see the failure
+                    cv_.notify_all();
+                }
+                cv_.wait(lk, [&] { return done_ || !tasks_.empty(); });
+                if (tasks_.empty()) return;
+                task = std::move(tasks_.front());
+                tasks_.pop_front();
+                if (err_ != cudaSuccess) continue;
+            }
+            e = task();
+        }
+    }
+    int device_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<cudaError_t()>> tasks_;
+    std::vector<int> marks_;
+    bool done_ = false;
+    cudaError_t err_ = cudaSuccess;
+    std::thread th_;
+};
+
+// Input copies of group d, then its event (issued by the copy thread).
+cudaError_t issue_stage_group(ndb_ctx *ctx, const ndb_job *jobs, const std::vector<ndb_job> &dj,
+                              const std::vector<int> &members, int d) {
+    for (int i : members) {
+        const cudaError_t e = cudaMemcpyAsync(const_cast<float *>(dj[i].coords), jobs[i].coords,
+                                              (size_t)jobs[i].n * d * sizeof(float), cudaMemcpyHostToDevice,
+                                              ctx->copy_stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaEventRecord(ctx->ev_grp[d], ctx->copy_stream);
+}
+
+// Output copies of finished jobs, after the event `done` the calling thread
+// recorded on the context's stream (issued by the copy thread).
+cudaError_t issue_unstage(ndb_ctx *ctx, const ndb_job *jobs, const std::vector<ndb_job> &dj,
+                          const std::vector<int> &which, cudaEvent_t done) {
+    cudaError_t e = cudaStreamWaitEvent(ctx->copy_stream, done, 0);
+    for (size_t q = 0; q < which.size() && e == cudaSuccess; ++q) {
+        const int i = which[q];
         const ndb_job &J = jobs[i];
         if (J.nn_out)
-            ck(ctx, cudaMemcpyAsync(J.nn_out, dj[i].nn_out, (size_t)J.n * sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                    ctx->copy_stream));
-        if (J.cluster_index_out)
-            ck(ctx, cudaMemcpyAsync(J.cluster_index_out, dj[i].cluster_index_out, (size_t)J.n * sizeof(int32_t),
-                                    cudaMemcpyDeviceToHost, ctx->copy_stream));
+            e = cudaMemcpyAsync(J.nn_out, dj[i].nn_out, (size_t)J.n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                ctx->copy_stream);
+        if (e == cudaSuccess && J.cluster_index_out)
+            e = cudaMemcpyAsync(J.cluster_index_out, dj[i].cluster_index_out, (size_t)J.n * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, ctx->copy_stream);
     }
+    return e;
 }
 
 }  // namespace
@@ -2060,7 +2234,11 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     ctx->stats = ndb_stats{};
     launch_counter() = 0;
     if (grow(ctx, ctx->small, kSmallBytes) != cudaSuccess) return NDB_ERR_OUT_OF_MEMORY;
-    if (cudaMemsetAsync(ctx->small.ptr, 0, kSmallBytes, ctx->stream) != cudaSuccess) return NDB_ERR_CUDA;
+    try {
+        fill_bytes(ctx, ctx->small.ptr, 0, kSmallBytes, ctx->stream);
+    } catch (const Fail &f) {
+        return f.st;
+    }
     ++launch_counter(), set_int_kernel<<<1, 1, 0, ctx->stream>>>(small_at<int>(ctx, kSmallErrOff) + 1,
                                                                  ctx->uf_max_steps);
     if (cudaGetLastError() != cudaSuccess) return NDB_ERR_CUDA;
@@ -2083,28 +2261,48 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
         if (J.n == 0) continue;
         groups[J.d].push_back((int)i);
     }
+    // the pipelines' small transfers: per job two job-table entries, a bounding box,
+    // its invalid count and four counters; per pipeline the stencil and some scalars
+    try {
+        ensure_mail(ctx, (size_t)n_jobs * (2 * sizeof(JobDev) + 2 * NDB_MAX_DIM * sizeof(int) + 5 * 8) +
+                             kMaxRows * sizeof(int4) + 16 * 1024);
+    } catch (const Fail &f) {
+        return f.st;
+    }
     // host buffers: inputs staged group by group on the copy stream, outputs back
     // group by group; the pipelines run on the device copies
     const bool host_io = !(flags & NDB_FLAG_DEVICE_PTRS) && ctx->copy_stream;
     std::vector<ndb_job> dj;
     ndb_job *work = jobs;
     uint32_t wflags = flags;
+    std::unique_ptr<CopyIssuer> io;  // issues the host copies from its own thread
     if (host_io) {
         try {
-            stage_batch(ctx, jobs, n_jobs, groups, dj);
+            plan_stage(ctx, jobs, n_jobs, groups, dj);
         } catch (const Fail &f) {
-            cudaStreamSynchronize(ctx->copy_stream);
             for (int d = 1; d <= NDB_MAX_DIM; ++d)  // every job that was to run carries the failure
                 for (int i : groups[d]) jobs[i].status = f.st;
             return f.st;
         }
         work = dj.data();
         wflags |= NDB_FLAG_DEVICE_PTRS;
+        io.reset(new CopyIssuer(ctx->device));
+        for (int d = 1; d <= NDB_MAX_DIM; ++d) {
+            if (groups[d].empty()) continue;
+            const std::vector<int> &members = groups[d];
+            io->push([ctx, jobs, &dj, &members, d] { return issue_stage_group(ctx, jobs, dj, members, d); });
+            io->mark(d);
+        }
     }
     std::vector<int> solo;
     for (int d = 1; d <= NDB_MAX_DIM; ++d) {
-        if (host_io && !groups[d].empty() && cudaStreamWaitEvent(ctx->stream, ctx->ev_grp[d], 0) != cudaSuccess) {
-            if (first == NDB_OK) first = NDB_ERR_CUDA;
+        if (host_io && !groups[d].empty()) {
+            // the group's input copies and their event are queued before the stream waits on it
+            if (!io->wait_mark(d) || cudaStreamWaitEvent(ctx->stream, ctx->ev_grp[d], 0) != cudaSuccess) {
+                if (first == NDB_OK) first = NDB_ERR_CUDA;
+                for (int i : groups[d]) dj[i].status = NDB_ERR_CUDA;
+                continue;
+            }
         }
         const size_t solo_before = solo.size();
         // pipelines of at most kMaxBatchPoints points
@@ -2140,13 +2338,14 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
             if (gs != NDB_OK && first == NDB_OK) first = gs;
         }
         if (host_io && !groups[d].empty()) {
-            std::vector<int> done;
+            auto done = std::make_shared<std::vector<int>>();
             for (int i : groups[d])
-                if (std::find(solo.begin() + solo_before, solo.end(), i) == solo.end()) done.push_back(i);
-            try {
-                unstage_jobs(ctx, jobs, dj, done);
-            } catch (const Fail &f) {
-                if (first == NDB_OK) first = f.st;
+                if (std::find(solo.begin() + solo_before, solo.end(), i) == solo.end()) done->push_back(i);
+            if (cudaEventRecord(ctx->ev_done[d], ctx->stream) != cudaSuccess) {
+                if (first == NDB_OK) first = NDB_ERR_CUDA;
+            } else if (!done->empty()) {
+                cudaEvent_t ev = ctx->ev_done[d];
+                io->push([ctx, jobs, &dj, done, ev] { return issue_unstage(ctx, jobs, dj, *done, ev); });
             }
         }
     }
@@ -2191,10 +2390,18 @@ extern "C" ndb_status ndb_b200_run_batched(ndb_ctx *ctx, ndb_job *jobs, int64_t 
     acc.solo_jobs = (int32_t)solo.size();
     ctx->stats = acc;
     if (host_io) {
-        try {
-            unstage_jobs(ctx, jobs, dj, solo);
-        } catch (const Fail &f) {
-            if (first == NDB_OK) first = f.st;
+        if (!solo.empty()) {
+            cudaEvent_t ev = ctx->ev_done[NDB_MAX_DIM + 1];
+            if (cudaEventRecord(ev, ctx->stream) != cudaSuccess) {
+                if (first == NDB_OK) first = NDB_ERR_CUDA;
+            } else {
+                io->push([ctx, jobs, &dj, &solo, ev] { return issue_unstage(ctx, jobs, dj, solo, ev); });
+            }
+        }
+        const cudaError_t ioe = io->finish();
+        if (ioe != cudaSuccess) {
+            ctx->last_cuda_error = cudaGetErrorString(ioe);
+            if (first == NDB_OK) first = ioe == cudaErrorMemoryAllocation ? NDB_ERR_OUT_OF_MEMORY : NDB_ERR_CUDA;
         }
         if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && first == NDB_OK) first = NDB_ERR_CUDA;
         for (int64_t i = 0; i < n_jobs; ++i) {

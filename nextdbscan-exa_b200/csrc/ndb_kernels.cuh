@@ -661,6 +661,10 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     unsigned long long *__restrict__ band_counter) {
     constexpr int P = Stride<D>::P;
     static_assert(!GRAM || D >= 8, "the Gram filter is built for d >= 8");
+    // d >= 8: each lane holds two candidates per step (64 per warp), so an owned
+    // point is read from shared memory once per two pairs and the two distance sums
+    // (each in the reference's order) are independent chains for the scheduler
+    constexpr int CH = D >= 8 ? 2 : 1;
     __shared__ __align__(16) float s_i[kCountWarps][kTile * P];
     __shared__ __align__(16) float s_a[kCountWarps][GRAM ? kTile * P : 4];  // centred points
     __shared__ float s_n[kCountWarps][GRAM ? kTile : 1];                     // their squared norms
@@ -724,10 +728,6 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) count_kernel(
     // is still filling (count below list_cap): both warp-uniform, updated per chunk
     unsigned act = __ballot_sync(kFull, lane < cnt);
     unsigned lst = nbr_list && list_cap > 0 ? act : 0u;
-    // d >= 8: each lane holds two candidates per step (64 per warp), so an owned
-    // point is read from shared memory once per two pairs and the two distance sums
-    // (each in the reference's order) are independent chains for the scheduler
-    constexpr int CH = D >= 8 ? 2 : 1;
     int row = 0;  // this lane's stencil row: its candidate index only grows
     for (int tb = 0; tb < total; tb += kWarp * CH) {
         int j[CH];
@@ -912,6 +912,22 @@ __global__ void iota_kernel(int32_t *__restrict__ a, int64_t n) {
 __global__ void fill_kernel(int32_t *__restrict__ a, int64_t n, int32_t v) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = v;
+}
+
+// bytes [0, bytes) of p set to v: n16 16-byte stores (p 16-byte aligned; 0 when it
+// is not), then the tail byte by byte
+__global__ void fill_bytes_kernel(uint8_t *__restrict__ p, size_t bytes, int64_t n16, uint8_t v) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t w = 0x01010101u * v;
+    for (int64_t i = t; i < n16; i += stride) reinterpret_cast<uint4 *>(p)[i] = make_uint4(w, w, w, w);
+    for (int64_t i = n16 * 16 + t; i < (int64_t)bytes; i += stride) p[i] = v;
+}
+
+// n words from src to dst (either may be mapped host memory)
+__global__ void copy_words_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, int64_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = src[i];
 }
 
 // Loads the core points of an item into shared memory (compacted); returns how many.
