@@ -134,6 +134,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "memory");
 }
 
+// acc | (bit when a <= b): an ordered compare (false for NaN) as a 0 / all-ones word,
+// merged under the column's bit by one three-input logic operation
+__device__ __forceinline__ unsigned or_if_le(unsigned acc, float a, float b, unsigned bit) {
+    unsigned m, r;
+    asm("set.le.u32.f32 %0, %1, %2;" : "=r"(m) : "f"(a), "f"(b));
+    asm("lop3.b32 %0, %1, %2, %3, 0xEA;" : "=r"(r) : "r"(m), "r"(bit), "r"(acc));  // (m & bit) | acc
+    return r;
+}
+
 // 32x32 bit-matrix transpose across a warp: lane l holds row l (bit c = column
 // c) on entry and column l (bit r = row r) on return.
 __device__ __forceinline__ unsigned transpose32(unsigned x, int lane) {
@@ -397,16 +406,23 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
                 tc_after_sync();
                 uint32_t g[32];
                 tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(pb * kN), g);
+                // every column is classified (no per-column branch) and the inactive
+                // ones are masked out afterwards; the norms come four per load
                 unsigned hb = 0, bb = 0;
 #pragma unroll
-                for (int c = 0; c < kN; ++c) {
-                    if ((act >> c) & 1u) {
-                        const float v = __fmaf_rn(-2.0f, __uint_as_float(g[c]), s_ni[c]);
-                        hb |= (v <= tlo_cur ? 1u : 0u) << c;
-                        bb |= (v <= thi_cur ? 1u : 0u) << c;
+                for (int q = 0; q < kN / 4; ++q) {
+                    const float4 n4 = reinterpret_cast<const float4 *>(s_ni)[q];
+                    const float nv[4] = {n4.x, n4.y, n4.z, n4.w};
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int c = 4 * q + r;
+                        const float v = __fmaf_rn(-2.0f, __uint_as_float(g[c]), nv[r]);
+                        hb = or_if_le(hb, v, tlo_cur, 1u << c);
+                        bb = or_if_le(bb, v, thi_cur, 1u << c);
                     }
                 }
-                bb &= ~hb;
+                hb &= act;
+                bb &= act & ~hb;
                 if constexpr (AUDIT) audit_tile<D>(s_x, s_ni, g, act, hb, bb, j_cur, nj_cur, xs, e2j, kap, audit);
                 if (__any_sync(kFull, bb != 0)) {
                     if (bb) {
