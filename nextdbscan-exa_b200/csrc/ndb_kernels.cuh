@@ -1421,7 +1421,10 @@ __global__ void cell_root_kernel(int64_t nv, const int32_t *__restrict__ pcell,
 // follow skip every candidate already under the same root.  With the early exit, the
 // count skips the cells of >= min_pts points of a same-cell-linked grid and records no
 // list there (skip_dense): those cells are joined by the near and cell passes.
-constexpr int kListUnions = 8;
+#ifndef NDB_LIST_UNIONS
+#define NDB_LIST_UNIONS 8
+#endif
+constexpr int kListUnions = NDB_LIST_UNIONS;  // a build-time choice
 __global__ void union_lists_kernel(int64_t nv, const int32_t *__restrict__ nn_sorted,
                                    const int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
                                    const uint8_t *__restrict__ core_sorted, int32_t *parent, int *err,

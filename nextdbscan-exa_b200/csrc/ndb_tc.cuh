@@ -34,6 +34,10 @@ constexpr int kThreads = 128;        // four warps, one per TMEM lane quadrant
 constexpr uint32_t kTmemCols = 64;   // two accumulator buffers
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr int kMinDim = 8;           // the kernel is built for d >= 8 (K padded to 8 or 16)
+// resident CTAs per SM the register allocation is sized for (a build-time choice)
+#ifndef NDB_TC_MIN_BLOCKS
+#define NDB_TC_MIN_BLOCKS 4
+#endif
 
 template <int D>
 struct KPad {
@@ -134,12 +138,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "memory");
 }
 
-// acc | (bit when a <= b): an ordered compare (false for NaN) as a 0 / all-ones word,
-// merged under the column's bit by one three-input logic operation
-__device__ __forceinline__ unsigned or_if_le(unsigned acc, float a, float b, unsigned bit) {
-    unsigned m, r;
-    asm("set.le.u32.f32 %0, %1, %2;" : "=r"(m) : "f"(a), "f"(b));
-    asm("lop3.b32 %0, %1, %2, %3, 0xEA;" : "=r"(r) : "r"(m), "r"(bit), "r"(acc));  // (m & bit) | acc
+// (acc << 1) | sign bit of x: one funnel shift appends a sign bit to a mask built
+// from the last column down, so that column c ends at bit c
+__device__ __forceinline__ unsigned push_sign(unsigned acc, float x) {
+    unsigned r;
+    asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(__float_as_uint(x)), "r"(acc));
     return r;
 }
 
@@ -248,7 +251,7 @@ __device__ __forceinline__ void audit_tile(const float *s_x, const float *s_ni, 
 }
 
 template <int D, bool AUDIT = false>
-__global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
+__global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts, int early,
     int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
@@ -406,23 +409,27 @@ __global__ void __launch_bounds__(kThreads, 4) count_tc_kernel(
                 tc_after_sync();
                 uint32_t g[32];
                 tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(pb * kN), g);
-                // every column is classified (no per-column branch) and the inactive
-                // ones are masked out afterwards; the norms come four per load
-                unsigned hb = 0, bb = 0;
+                // Every column is classified (no per-column branch; inactive ones are
+                // masked out afterwards) from the sign of tlo - v and thi - v: with
+                // finite operands and rounding to nearest the difference is >= +0
+                // exactly when v <= the bound (neither bound is ever -0, so no -0
+                // difference arises), and the sign bits are appended to two masks
+                // by funnel shifts.  The norms come four per shared load.
+                unsigned mlo = 0, mhi = 0;  // bit c: v_c > tlo, v_c > thi
 #pragma unroll
-                for (int q = 0; q < kN / 4; ++q) {
+                for (int q = kN / 4 - 1; q >= 0; --q) {
                     const float4 n4 = reinterpret_cast<const float4 *>(s_ni)[q];
                     const float nv[4] = {n4.x, n4.y, n4.z, n4.w};
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) {
+                    for (int r = 3; r >= 0; --r) {
                         const int c = 4 * q + r;
                         const float v = __fmaf_rn(-2.0f, __uint_as_float(g[c]), nv[r]);
-                        hb = or_if_le(hb, v, tlo_cur, 1u << c);
-                        bb = or_if_le(bb, v, thi_cur, 1u << c);
+                        mlo = push_sign(mlo, __fsub_rn(tlo_cur, v));
+                        mhi = push_sign(mhi, __fsub_rn(thi_cur, v));
                     }
                 }
-                hb &= act;
-                bb &= act & ~hb;
+                unsigned hb = ~mlo & act;
+                unsigned bb = ~mhi & mlo & act;
                 if constexpr (AUDIT) audit_tile<D>(s_x, s_ni, g, act, hb, bb, j_cur, nj_cur, xs, e2j, kap, audit);
                 if (__any_sync(kFull, bb != 0)) {
                     if (bb) {
