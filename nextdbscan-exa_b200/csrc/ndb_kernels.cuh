@@ -1422,7 +1422,7 @@ __global__ void cell_root_kernel(int64_t nv, const int32_t *__restrict__ pcell,
 // count skips the cells of >= min_pts points of a same-cell-linked grid and records no
 // list there (skip_dense): those cells are joined by the near and cell passes.
 #ifndef NDB_LIST_UNIONS
-#define NDB_LIST_UNIONS 8
+#define NDB_LIST_UNIONS 16
 #endif
 constexpr int kListUnions = NDB_LIST_UNIONS;  // a build-time choice
 __global__ void union_lists_kernel(int64_t nv, const int32_t *__restrict__ nn_sorted,
