@@ -74,8 +74,13 @@ __device__ __forceinline__ uint64_t desc_kmajor(uint32_t addr, uint32_t lbo, uin
 
 // Instruction descriptor of kind::tf32: FP32 accumulator (bits 4-5 = 1), A and B
 // TF32 (bits 7-9, 10-12 = 2), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kN >> 3) << 17) |
-                            ((uint32_t)(kM >> 4) << 24);
+// N is 32 (a whole item) or 16 (its still-active points, packed; M = 128 allows N
+// in steps of 16).
+__host__ __device__ constexpr uint32_t idesc_tf32(int n) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+}
+constexpr uint32_t kIdesc = idesc_tf32(kN);
+constexpr uint32_t kIdescNarrow = idesc_tf32(kN / 2);
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -110,11 +115,12 @@ __device__ __forceinline__ void tmem_relinquish() {
 __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate,
+                                         uint32_t idesc = kIdesc) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -137,6 +143,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "r"(taddr)
         : "memory");
 }
+// The first 16 of them (the packed form, N = 16).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
 
 // (acc << 1) | sign bit of x: one funnel shift appends a sign bit to a mask built
 // from the last column down, so that column c ends at bit c
@@ -144,6 +161,41 @@ __device__ __forceinline__ unsigned push_sign(unsigned acc, float x) {
     unsigned r;
     asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(__float_as_uint(x)), "r"(acc));
     return r;
+}
+
+// Classification of the first NC accumulator columns of this thread's TMEM lane (one
+// candidate j) against its bounds tlo, thi of the comparison value v_c = n_c - 2 g_c.
+// v is formed negated, two columns per packed FMA: w_c = 2 g_c + (-n_c) is -v_c
+// exactly (one rounding to nearest, which is symmetric); tlo + w_c = RN(tlo - v_c),
+// two columns per packed add.  With finite operands the sum is >= +0 exactly when
+// v_c <= tlo (neither bound is ever -0), so bit c of mlo (mhi) is set when v_c > tlo
+// (v_c > thi); one funnel shift per bound appends the sign bit, last column first.
+// Bits at and above NC are 0.  s_nneg holds -n_c.
+template <int NC>
+__device__ __forceinline__ void classify(const uint32_t (&g)[32], const float *s_nneg, float tlo, float thi,
+                                         unsigned &mlo, unsigned &mhi) {
+    const float2 two = make_float2(2.0f, 2.0f), lo2 = make_float2(tlo, tlo), hi2 = make_float2(thi, thi);
+    unsigned ml = 0, mh = 0;
+#pragma unroll
+    for (int q = NC / 4 - 1; q >= 0; --q) {
+        const float4 n4 = reinterpret_cast<const float4 *>(s_nneg)[q];
+        const float2 w1 = __ffma2_rn(make_float2(__uint_as_float(g[4 * q + 2]), __uint_as_float(g[4 * q + 3])), two,
+                                     make_float2(n4.z, n4.w));
+        const float2 w0 = __ffma2_rn(make_float2(__uint_as_float(g[4 * q + 0]), __uint_as_float(g[4 * q + 1])), two,
+                                     make_float2(n4.x, n4.y));
+        const float2 l1 = __fadd2_rn(lo2, w1), h1 = __fadd2_rn(hi2, w1);
+        const float2 l0 = __fadd2_rn(lo2, w0), h0 = __fadd2_rn(hi2, w0);
+        ml = push_sign(ml, l1.y);
+        mh = push_sign(mh, h1.y);
+        ml = push_sign(ml, l1.x);
+        mh = push_sign(mh, h1.x);
+        ml = push_sign(ml, l0.y);
+        mh = push_sign(mh, h0.y);
+        ml = push_sign(ml, l0.x);
+        mh = push_sign(mh, h0.x);
+    }
+    mlo = ml;
+    mhi = mh;
 }
 
 // 32x32 bit-matrix transpose across a warp: lane l holds row l (bit c = column
@@ -170,19 +222,32 @@ __device__ __forceinline__ void store_row(uint32_t *tile, int rows, int r, const
             make_uint4(v[4 * q + 0], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
 }
 
-// x - o, split into TF32 hi + lo, and |x - o|^2 (FP32)
+// a = x - o, split into TF32 hi + lo, and |a|^2 (FP32), two dimensions per packed
+// instruction; no = -o.  a = RN(x + (-o)) and lo = tf32(RN(a - hi)) (exact: a - hi
+// fits in FP32) are the scalar values; the norm is two interleaved FMA chains added
+// at the end, within the K u |a|^2 the error bound allows for it.  Padded dimensions
+// (k >= D) are zero.
 template <int D, int KP>
-__device__ __forceinline__ float centre_split(const float (&x)[D], const float (&o)[D], uint32_t (&hi)[KP],
+__device__ __forceinline__ float centre_split(const float (&x)[D], const float (&no)[D], uint32_t (&hi)[KP],
                                               uint32_t (&lo)[KP]) {
-    float n = 0.0f;
+    float2 n2 = make_float2(0.0f, 0.0f);
 #pragma unroll
-    for (int k = 0; k < KP; ++k) {
-        const float a = k < D ? __fsub_rn(x[k], o[k]) : 0.0f;
-        hi[k] = tf32_rna(a);
-        lo[k] = tf32_rna(__fsub_rn(a, __uint_as_float(hi[k])));
-        n = __fmaf_rn(a, a, n);
+    for (int k = 0; k < KP; k += 2) {
+        if (k >= D) {
+            hi[k] = lo[k] = hi[k + 1] = lo[k + 1] = 0u;
+            continue;
+        }
+        const float2 a = k + 1 < D ? __fadd2_rn(make_float2(x[k], x[k + 1]), make_float2(no[k], no[k + 1]))
+                                   : make_float2(__fadd_rn(x[k], no[k]), 0.0f);
+        hi[k] = tf32_rna(a.x);
+        hi[k + 1] = k + 1 < D ? tf32_rna(a.y) : 0u;
+        const float2 l = __ffma2_rn(make_float2(__uint_as_float(hi[k]), __uint_as_float(hi[k + 1])),
+                                    make_float2(-1.0f, -1.0f), a);
+        lo[k] = tf32_rna(l.x);
+        lo[k + 1] = k + 1 < D ? tf32_rna(l.y) : 0u;
+        n2 = __ffma2_rn(a, a, n2);
     }
-    return n;
+    return __fadd_rn(n2.x, n2.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -250,6 +315,21 @@ __device__ __forceinline__ void audit_tile(const float *s_x, const float *s_ni, 
     }
 }
 
+// Position of the (k+1)-th set bit of m (k < popc(m)): binary search on popcounts.
+__device__ __forceinline__ int nth_set_bit(unsigned m, int k) {
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) {
+        const int c = __popc(m & ((1u << w) - 1u));
+        if (k >= c) {
+            k -= c;
+            m >>= w;
+            pos += w;
+        }
+    }
+    return pos;
+}
+
 template <int D, bool AUDIT = false>
 __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
@@ -260,10 +340,14 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
     const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr,
     unsigned long long *__restrict__ audit = nullptr) {
     constexpr int KP = KPad<D>::v, P = Stride<D>::P, KC = KP / 4;
+    static_assert(P % 4 == 0, "point rows are copied as float4");
+    // The item's points live in one of two sets: set 0 as staged, set 1 with the
+    // still-active points packed into the first 16 columns (see the packing below).
     __shared__ __align__(1024) uint32_t s_a[2][2][KC * kM * 4];  // [buffer][hi, lo] candidate tiles
-    __shared__ __align__(128) uint32_t s_b[2][KC * kN * 4];      // [hi, lo] the item's points
-    __shared__ __align__(16) float s_x[kN * P];                   // the item's points as stored
-    __shared__ __align__(16) float s_ni[kN];
+    __shared__ __align__(128) uint32_t s_b[2][2][KC * kN * 4];   // [set][hi, lo] the item's points
+    __shared__ __align__(16) float s_x[2][kN * P];                // [set] the item's points as stored
+    __shared__ __align__(16) float s_ni[2][kN];                   // [set] |x_c - o|^2
+    __shared__ __align__(16) float s_nneg[2][kN];                 // [set] -|x_c - o|^2
     __shared__ int s_j[2][kM];
     __shared__ int s_part[2][4][kN];
     __shared__ int s_listn[kN];
@@ -309,20 +393,23 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
             mp = J.min_pts;
             lc = J.list_cap;
         }
-        float o[D];
+        float o[D];  // the item's first point, negated: the centre of its Gram tiles
         load_point<D>(xs, p0, o);
+#pragma unroll
+        for (int k = 0; k < D; ++k) o[k] = -o[k];
         if (warp == 0) {
             gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, s_rt, lane);
             s_listn[lane] = 0;
         } else if (warp == 1) {
             float x[D];
             load_point<D>(xs, p0 + min(lane, cnt - 1), x);
-            store_point_smem<D>(s_x + lane * P, x);
+            store_point_smem<D>(s_x[0] + lane * P, x);
             uint32_t hi[KP], lo[KP];
             const float n = centre_split<D, KP>(x, o, hi, lo);
-            store_row<KP>(s_b[0], kN, lane, hi);
-            store_row<KP>(s_b[1], kN, lane, lo);
-            s_ni[lane] = n;
+            store_row<KP>(s_b[0][0], kN, lane, hi);
+            store_row<KP>(s_b[0][1], kN, lane, lo);
+            s_ni[0][lane] = n;
+            s_nneg[0][lane] = -n;
             float nm = lane < cnt ? n : 0.0f;
 #pragma unroll
             for (int s = 16; s > 0; s >>= 1) nm = fmaxf(nm, __shfl_xor_sync(kFull, nm, s));
@@ -336,6 +423,10 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
         const int n_tiles = (total + kM - 1) / kM;
         unsigned act = cnt >= kN ? kFull : ((1u << cnt) - 1u);
         int run = 0, totals = 0;  // lane c: this warp's hits of column c; all warps' hits after the last tile
+        // Columns: column c holds item point pcol (of lane c) in point set `set`; ncols
+        // columns hold points.  narrow: the MMA computes 16 columns (N = 16).
+        int set = 0, ncols = cnt, pcol = lane;
+        bool narrow = false;
 
         // One candidate row per thread.  fetch: the row's point index (a cursor over
         // the stencil rows, advanced as the tile index grows) and its coordinates,
@@ -374,15 +465,16 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
             const int b = t & 1;
             const uint32_t d = tmem + (uint32_t)(b * kN);
             const uint32_t ah = smem_u32(s_a[b][0]), al = smem_u32(s_a[b][1]);
-            const uint32_t bh = smem_u32(s_b[0]), bl = smem_u32(s_b[1]);
+            const uint32_t bh = smem_u32(s_b[set][0]), bl = smem_u32(s_b[set][1]);
+            const uint32_t id = narrow ? kIdescNarrow : kIdesc;
 #pragma unroll
             for (int s = 0; s < KP / 8; ++s) {
                 const uint32_t ao = (uint32_t)(s * 2 * kM * 16), bo = (uint32_t)(s * 2 * kN * 16);
                 const uint64_t dah = desc_kmajor(ah + ao, kM * 16, 128), dal = desc_kmajor(al + ao, kM * 16, 128);
                 const uint64_t dbh = desc_kmajor(bh + bo, kN * 16, 128), dbl = desc_kmajor(bl + bo, kN * 16, 128);
-                mma_tf32(d, dah, dbh, s > 0 ? 1u : 0u);
-                mma_tf32(d, dah, dbl, 1u);
-                mma_tf32(d, dal, dbh, 1u);
+                mma_tf32(d, dah, dbh, s > 0 ? 1u : 0u, id);
+                mma_tf32(d, dah, dbl, 1u, id);
+                mma_tf32(d, dal, dbh, 1u, id);
             }
             mma_commit(&s_bar[b]);
         };
@@ -408,29 +500,22 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
                 pending &= ~(1u << pb);
                 tc_after_sync();
                 uint32_t g[32];
-                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(pb * kN), g);
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(pb * kN);
                 // Every column is classified (no per-column branch; inactive ones are
-                // masked out afterwards) from the sign of tlo - v and thi - v: with
-                // finite operands and rounding to nearest the difference is >= +0
-                // exactly when v <= the bound (neither bound is ever -0, so no -0
-                // difference arises), and the sign bits are appended to two masks
-                // by funnel shifts.  The norms come four per shared load.
-                unsigned mlo = 0, mhi = 0;  // bit c: v_c > tlo, v_c > thi
-#pragma unroll
-                for (int q = kN / 4 - 1; q >= 0; --q) {
-                    const float4 n4 = reinterpret_cast<const float4 *>(s_ni)[q];
-                    const float nv[4] = {n4.x, n4.y, n4.z, n4.w};
-#pragma unroll
-                    for (int r = 3; r >= 0; --r) {
-                        const int c = 4 * q + r;
-                        const float v = __fmaf_rn(-2.0f, __uint_as_float(g[c]), nv[r]);
-                        mlo = push_sign(mlo, __fsub_rn(tlo_cur, v));
-                        mhi = push_sign(mhi, __fsub_rn(thi_cur, v));
-                    }
+                // masked out afterwards): 16 columns once the item is packed, else 32.
+                unsigned mlo, mhi;  // bit c: v_c > tlo, v_c > thi
+                if (narrow) {
+                    tmem_ld16(taddr, g);
+                    classify<kN / 2>(g, s_nneg[1], tlo_cur, thi_cur, mlo, mhi);
+                } else {
+                    tmem_ld32(taddr, g);
+                    classify<kN>(g, s_nneg[set], tlo_cur, thi_cur, mlo, mhi);
                 }
+                const float *sx = s_x[set];
                 unsigned hb = ~mlo & act;
                 unsigned bb = ~mhi & mlo & act;
-                if constexpr (AUDIT) audit_tile<D>(s_x, s_ni, g, act, hb, bb, j_cur, nj_cur, xs, e2j, kap, audit);
+                if constexpr (AUDIT)
+                    audit_tile<D>(sx, s_ni[set], g, act, hb, bb, j_cur, nj_cur, xs, e2j, kap, audit);
                 if (__any_sync(kFull, bb != 0)) {
                     if (bb) {
                         float xj[D];
@@ -439,7 +524,7 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
                         for (unsigned m = bb; m; m &= m - 1) {
                             const int c = __ffs(m) - 1;
                             float xi[D];
-                            load_point_smem<D>(s_x + c * P, xi);
+                            load_point_smem<D>(sx + c * P, xi);
                             if (in_range<D>(xi, xj, e2j)) hb |= 1u << c;
                         }
                     }
@@ -451,7 +536,7 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
                     if (nbr_list && h && totals < lc) {
                         int slot = atomicAdd(&s_listn[lane], h);
                         for (unsigned m = cm; m && slot < lc; m &= m - 1, ++slot)
-                            nbr_list[(int64_t)(p0 + lane) * list_stride + slot] = s_j[pb][warp * 32 + __ffs(m) - 1];
+                            nbr_list[(int64_t)(p0 + pcol) * list_stride + slot] = s_j[pb][warp * 32 + __ffs(m) - 1];
                     }
                 }
                 s_part[t & 1][warp][lane] = run;
@@ -467,9 +552,46 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
             tc_after_sync();
             if (s_abort) break;
             totals = s_part[t & 1][0][lane] + s_part[t & 1][1][lane] + s_part[t & 1][2][lane] + s_part[t & 1][3][lane];
-            if (early) act = __ballot_sync(kFull, lane < cnt && totals < mp);
+            if (early) act = __ballot_sync(kFull, lane < ncols && totals < mp);
             if (early && !act) break;
             if (t < n_tiles) {
+                // Packing (early exit only, once per item): when at most 16 columns are
+                // still active, they move to the first 16 columns of point set 1 and the
+                // MMAs compute N = 16 from then on, halving the classification.  A finished
+                // column's count is final: it is written out here.  No MMA is in flight
+                // (the last one was waited for above), so set 1 may be written.
+                if (early && !narrow && __popc(act) <= kN / 2) {
+                    const int nk = __popc(act);
+                    if (warp == 0 && lane < ncols && !((act >> lane) & 1u)) nn_sorted[p0 + pcol] = totals;
+                    const int src = lane < nk ? nth_set_bit(act, lane) : lane;
+                    run = __shfl_sync(kFull, run, src);
+                    totals = __shfl_sync(kFull, totals, src);
+                    pcol = __shfl_sync(kFull, pcol, src);
+                    if (warp == 0) {
+                        const int ln = s_listn[src];
+                        __syncwarp();
+                        s_listn[lane] = ln;
+                    } else if (warp == 1 && lane < nk) {
+#pragma unroll
+                        for (int q = 0; q < KC; ++q)
+#pragma unroll
+                            for (int h = 0; h < 2; ++h)
+                                *reinterpret_cast<uint4 *>(&s_b[1][h][(q * kN + lane) * 4]) =
+                                    *reinterpret_cast<const uint4 *>(&s_b[0][h][(q * kN + src) * 4]);
+#pragma unroll
+                        for (int q = 0; q < P / 4; ++q)
+                            *reinterpret_cast<float4 *>(&s_x[1][lane * P + 4 * q]) =
+                                *reinterpret_cast<const float4 *>(&s_x[0][src * P + 4 * q]);
+                        s_ni[1][lane] = s_ni[0][src];
+                        s_nneg[1][lane] = s_nneg[0][src];
+                        fence_async_smem();
+                    }
+                    set = 1;
+                    narrow = true;
+                    ncols = nk;
+                    act = (1u << nk) - 1u;
+                    __syncthreads();
+                }
                 if (tid == 0) issue(t);
                 pending |= 1u << (t & 1);
                 j_cur = j_nxt;
@@ -479,7 +601,7 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
             }
         }
         if (s_abort) break;
-        if (warp == 0 && lane < cnt) nn_sorted[p0 + lane] = totals;
+        if (warp == 0 && lane < ncols) nn_sorted[p0 + pcol] = totals;
     }
     // MMAs still in flight after an abort: wait for them (bounded) before freeing TMEM
     for (int b = 0; b < 2; ++b)
