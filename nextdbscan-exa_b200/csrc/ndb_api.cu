@@ -59,8 +59,9 @@ struct ndb_ctx {
     DevBuf sort_hist, scan_scratch, small;  // small: counters, bbox, scalars
     // batched runs: job table, per-job bounding boxes, cell -> job, per-job counters
     DevBuf jobs_dev, batch_bbox, cell_job, job_counters;
-    // items split between the tensor-core count (full items) and the exact one
-    DevBuf items_split;
+    // items split between the tensor-core count (full items) and the exact one, and
+    // the tensor count's per-item records
+    DevBuf items_split, tc_rec;
     // caller's core ids of ndb_b200_assign_border (host inputs)
     DevBuf ids_in;
     // batched runs on host buffers: every job's coordinates and outputs on the device
@@ -99,7 +100,7 @@ struct ndb_ctx {
                           &parent,      &comp_min,    &sort_hist,   &scan_scratch, &small,      &hash_keys,
                           &hash_vals,   &nbr_list,    &jobs_dev,    &batch_bbox,  &cell_job,    &job_counters,
                           &items_split, &col_range,   &ids_in,      &batch_in,    &batch_nn,    &batch_ci,
-                          &load_box};
+                          &load_box,    &tc_rec};
         for (DevBuf *b : bufs) f(*b);
     }
     size_t held_bytes() {
@@ -645,17 +646,29 @@ void launch_count_tc(ndb_ctx *ctx, int64_t n_items, const int2 *items, const int
         unsigned long long *counters = small_at<unsigned long long>(ctx, kSmallCountersOff);
         unsigned int *work = reinterpret_cast<unsigned int *>(counters + 6);
         fill_bytes(ctx, work, 0, sizeof(unsigned long long), st);
-        const unsigned grid = (unsigned)std::min<int64_t>(n_items, (int64_t)ctx->sm_count * 4);
+        // the items' records (stencil rows as point ranges), which the kernel fetches
+        // one item ahead by bulk copies; without room for them (a memory cap, the
+        // allocation-free entry point) the kernel gathers the rows itself
+        int2 *rec = nullptr;
+        if (n_items_dev && grow(ctx, ctx->tc_rec, (size_t)n_items * tc::kRecBytes) == cudaSuccess) {
+            rec = ctx->tc_rec.as<int2>();
+            ++launch_counter(), tc::tc_records_kernel<<<blocks_for(n_items * kWarp), kBlock, 0, st>>>(
+                items, n_items_dev, cell_start, nbr, n_rows, cell_job, rec);
+            ck(ctx, cudaGetLastError());
+        } else {
+            cudaGetLastError();  // a refused or failed allocation leaves no error behind
+        }
+        const unsigned grid = (unsigned)std::min<int64_t>(n_items, (int64_t)ctx->sm_count * tc::TcBlocks<D>::v);
         if (audit)
             ++launch_counter(), tc::count_tc_kernel<D, true><<<grid, tc::kThreads, 0, st>>>(
                 items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, early ? 1 : 0, nn_sorted, list, list_cap,
                 list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job,
-                n_items_dev, counters + 8);
+                n_items_dev, counters + 8, rec);
         else
             ++launch_counter(), tc::count_tc_kernel<D><<<grid, tc::kThreads, 0, st>>>(
                 items, n_items, cell_start, nbr, n_rows, xs, e2, min_pts, early ? 1 : 0, nn_sorted, list, list_cap,
                 list_stride, counters + 2, counters + 5, work, small_at<int>(ctx, kSmallErrOff), jobs, cell_job,
-                n_items_dev);
+                n_items_dev, nullptr, rec);
         ck(ctx, cudaGetLastError());
     } else {
         throw Fail{NDB_ERR_INVALID_ARGUMENT};

@@ -34,10 +34,25 @@ constexpr int kThreads = 128;        // four warps, one per TMEM lane quadrant
 constexpr uint32_t kTmemCols = 64;   // two accumulator buffers
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr int kMinDim = 8;           // the kernel is built for d >= 8 (K padded to 8 or 16)
-// resident CTAs per SM the register allocation is sized for (a build-time choice)
+// resident CTAs per SM the register allocation is sized for (a build-time choice):
+// d > 8 (48 KB of shared memory per CTA) and d = 8 (25.5 KB)
 #ifndef NDB_TC_MIN_BLOCKS
 #define NDB_TC_MIN_BLOCKS 4
 #endif
+#ifndef NDB_TC_MIN_BLOCKS_8
+#define NDB_TC_MIN_BLOCKS_8 5
+#endif
+template <int D>
+struct TcBlocks {
+    static constexpr int v = D <= 8 ? NDB_TC_MIN_BLOCKS_8 : NDB_TC_MIN_BLOCKS;
+};
+
+// Per-item record of the tensor count (tc_records_kernel), fetched one item ahead
+// by a bulk copy: int2 slot 0 = (cell, first point), slot 1 + r = (first point,
+// length) of stencil row r (r < 32), slot 33 = (points of the item, job or -1).
+// 34 slots = 272 bytes, a multiple of 16.
+constexpr int kRecSlots = 34;
+constexpr uint32_t kRecBytes = kRecSlots * 8;
 
 template <int D>
 struct KPad {
@@ -102,6 +117,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return false;
 }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// One bulk copy (the TMA's untiled form) of `bytes` (a multiple of 16; both addresses
+// 16-byte aligned) from this GPU's global memory into this CTA's shared memory,
+// completing on the mbarrier with a transaction count.  No multicast.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
 __device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
@@ -330,15 +356,39 @@ __device__ __forceinline__ int nth_set_bit(unsigned m, int k) {
     return pos;
 }
 
+// The records of the items in items[0, *n_items): one warp per item.
+__global__ void tc_records_kernel(const int2 *__restrict__ items, const uint32_t *__restrict__ n_items,
+                                  const int32_t *__restrict__ cell_start, const int2 *__restrict__ nbr, int n_rows,
+                                  const int32_t *__restrict__ cell_job, int2 *__restrict__ rec) {
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (int64_t)*n_items) return;
+    const int2 it = items[w];
+    int2 *r = rec + w * kRecSlots;
+    if (lane < n_rows) {
+        const int2 cr = nbr[(int64_t)it.x * n_rows + lane];
+        int2 v = make_int2(0, 0);
+        if (cr.x < cr.y) {
+            const int a = cell_start[cr.x];
+            v = make_int2(a, cell_start[cr.y] - a);
+        }
+        r[1 + lane] = v;
+    }
+    if (lane == 0) {
+        r[0] = it;
+        r[33] = make_int2(min(kN, cell_start[it.x + 1] - it.y), cell_job ? cell_job[it.x] : -1);
+    }
+}
+
 template <int D, bool AUDIT = false>
-__global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
+__global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
     const int2 *__restrict__ items, int64_t n_items, const int32_t *__restrict__ cell_start,
     const int2 *__restrict__ nbr, int n_rows, const float *__restrict__ xs, float e2, int min_pts, int early,
     int32_t *__restrict__ nn_sorted, int32_t *__restrict__ nbr_list, int list_cap, int list_stride,
     unsigned long long *__restrict__ pair_counter, unsigned long long *__restrict__ band_counter,
     unsigned int *__restrict__ work, int *__restrict__ err, const JobDev *__restrict__ jobs,
     const int32_t *__restrict__ cell_job, const uint32_t *__restrict__ n_items_dev = nullptr,
-    unsigned long long *__restrict__ audit = nullptr) {
+    unsigned long long *__restrict__ audit = nullptr, const int2 *__restrict__ rec = nullptr) {
     constexpr int KP = KPad<D>::v, P = Stride<D>::P, KC = KP / 4;
     static_assert(P % 4 == 0, "point rows are copied as float4");
     // The item's points live in one of two sets: set 0 as staged, set 1 with the
@@ -352,7 +402,9 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
     __shared__ int s_part[2][4][kN];
     __shared__ int s_listn[kN];
     __shared__ RowTable s_rt;
+    __shared__ __align__(16) int2 s_rec[2][kRecSlots];  // [slot] the records of this item and the next
     __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ __align__(8) uint64_t s_rbar[2];  // [slot] record copy complete
     __shared__ uint32_t s_tmem;
     __shared__ int s_item, s_abort;
     __shared__ float s_nmax;
@@ -365,6 +417,8 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
+        mbar_init(&s_rbar[0], 1);
+        mbar_init(&s_rbar[1], 1);
         fence_mbar_init();
         s_abort = 0;
     }
@@ -377,18 +431,63 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
     unsigned long long pairs = 0, band = 0;
     const float kap = kappa<KP>();
 
-    for (;;) {
-        if (tid == 0) s_item = (int)atomicAdd(work, 1u);
+    // Items are claimed one ahead (tid 0): the claim of the next item and, with
+    // records, the bulk copy of its record are issued when this item starts, so
+    // neither the work counter's round trip nor the record's dependent loads lie on
+    // the item's critical path.  Slot k & 1 holds item k's record.
+    int64_t cur = 0, nxt = 0;
+    uint32_t rphase = 0, rpend = 0;  // per slot: parity of its next completion; copies not yet waited for
+    if (tid == 0) {
+        cur = (int64_t)atomicAdd(work, 1u);
+        if (rec && cur < n_items) {
+            bulk_load(s_rec[0], rec + cur * kRecSlots, kRecBytes, &s_rbar[0]);
+            rpend |= 1u;
+        }
+        nxt = (int64_t)atomicAdd(work, 1u);
+    }
+    for (int k_item = 0;; ++k_item) {
+        const int slot = k_item & 1;
+        if (tid == 0) {
+            s_item = (int)(cur < n_items ? cur : n_items);
+            if (rec && nxt < n_items) {
+                // the other slot was last read before the previous item's setup barrier
+                fence_async_smem();
+                bulk_load(s_rec[slot ^ 1], rec + nxt * kRecSlots, kRecBytes, &s_rbar[slot ^ 1]);
+                rpend |= 1u << (slot ^ 1);
+            }
+            cur = nxt;
+            nxt = (int64_t)atomicAdd(work, 1u);
+        }
         __syncthreads();
         const int64_t item_id = s_item;
         if (item_id >= n_items || s_abort) break;
-        const int2 item = items[item_id];
+        int2 item;
+        int cnt, jb = -1;
+        if (rec) {
+            const bool ok = mbar_wait(&s_rbar[slot], (rphase >> slot) & 1u);
+            rphase ^= 1u << slot;
+            rpend &= ~(1u << slot);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) {
+                    s_abort = 1;
+                    atomicExch(err, 2);
+                }
+                break;
+            }
+            item = s_rec[slot][0];
+            const int2 t = s_rec[slot][33];
+            cnt = t.x;
+            jb = t.y;
+        } else {
+            item = items[item_id];
+            cnt = min(kN, cell_start[item.x + 1] - item.y);
+            if (jobs) jb = cell_job[item.x];
+        }
         const int cell = item.x, p0 = item.y;
-        const int cnt = min(kN, cell_start[cell + 1] - p0);
         float e2j = e2;
         int mp = min_pts, lc = list_cap;
         if (jobs) {
-            const JobDev &J = jobs[cell_job[cell]];
+            const JobDev &J = jobs[jb];
             e2j = J.e2;
             mp = J.min_pts;
             lc = J.list_cap;
@@ -398,7 +497,12 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
 #pragma unroll
         for (int k = 0; k < D; ++k) o[k] = -o[k];
         if (warp == 0) {
-            gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, s_rt, lane);
+            if (rec) {
+                const int2 rw = lane < n_rows ? s_rec[slot][1 + lane] : make_int2(0, 0);
+                build_rows(rw.x, rw.y, n_rows, s_rt, lane);
+            } else {
+                gather_rows<false>(nbr + (int64_t)cell * n_rows, n_rows, cell_start, 0, s_rt, lane);
+            }
             s_listn[lane] = 0;
         } else if (warp == 1) {
             float x[D];
@@ -603,9 +707,13 @@ __global__ void __launch_bounds__(kThreads, NDB_TC_MIN_BLOCKS) count_tc_kernel(
         if (s_abort) break;
         if (warp == 0 && lane < ncols) nn_sorted[p0 + pcol] = totals;
     }
-    // MMAs still in flight after an abort: wait for them (bounded) before freeing TMEM
+    // MMAs still in flight after an abort: wait for them (bounded) before freeing TMEM;
+    // record copies still in flight (issued by tid 0): wait for them before exiting
     for (int b = 0; b < 2; ++b)
         if ((pending >> b) & 1u) mbar_wait(&s_bar[b], (phase >> b) & 1u);
+    if (tid == 0)
+        for (int b = 0; b < 2; ++b)
+            if ((rpend >> b) & 1u) mbar_wait(&s_rbar[b], (rphase >> b) & 1u);
     tc_before_sync();
     __syncthreads();
     if (warp == 0) {
