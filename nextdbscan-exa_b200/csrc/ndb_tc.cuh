@@ -35,9 +35,10 @@ constexpr uint32_t kTmemCols = 64;   // two accumulator buffers
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr int kMinDim = 8;           // the kernel is built for d >= 8 (K padded to 8 or 16)
 // resident CTAs per SM the register allocation is sized for (a build-time choice):
-// d > 8 (48 KB of shared memory per CTA) and d = 8 (25.5 KB)
+// d > 8 (42 KB of shared memory per CTA; 5 measured 2 % faster than 4 on the 16-D
+// batch, at 96 registers) and d = 8 (23 KB)
 #ifndef NDB_TC_MIN_BLOCKS
-#define NDB_TC_MIN_BLOCKS 4
+#define NDB_TC_MIN_BLOCKS 5
 #endif
 #ifndef NDB_TC_MIN_BLOCKS_8
 #define NDB_TC_MIN_BLOCKS_8 5
@@ -391,13 +392,11 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
     unsigned long long *__restrict__ audit = nullptr, const int2 *__restrict__ rec = nullptr) {
     constexpr int KP = KPad<D>::v, P = Stride<D>::P, KC = KP / 4;
     static_assert(P % 4 == 0, "point rows are copied as float4");
-    // The item's points live in one of two sets: set 0 as staged, set 1 with the
-    // still-active points packed into the first 16 columns (see the packing below).
     __shared__ __align__(1024) uint32_t s_a[2][2][KC * kM * 4];  // [buffer][hi, lo] candidate tiles
-    __shared__ __align__(128) uint32_t s_b[2][2][KC * kN * 4];   // [set][hi, lo] the item's points
-    __shared__ __align__(16) float s_x[2][kN * P];                // [set] the item's points as stored
-    __shared__ __align__(16) float s_ni[2][kN];                   // [set] |x_c - o|^2
-    __shared__ __align__(16) float s_nneg[2][kN];                 // [set] -|x_c - o|^2
+    __shared__ __align__(128) uint32_t s_b[2][KC * kN * 4];      // [hi, lo] the item's points
+    __shared__ __align__(16) float s_x[kN * P];                   // the item's points as stored
+    __shared__ __align__(16) float s_ni[kN];                      // |x_c - o|^2
+    __shared__ __align__(16) float s_nneg[kN];                    // -|x_c - o|^2
     __shared__ int s_j[2][kM];
     __shared__ int s_part[2][4][kN];
     __shared__ int s_listn[kN];
@@ -507,13 +506,13 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
         } else if (warp == 1) {
             float x[D];
             load_point<D>(xs, p0 + min(lane, cnt - 1), x);
-            store_point_smem<D>(s_x[0] + lane * P, x);
+            store_point_smem<D>(s_x + lane * P, x);
             uint32_t hi[KP], lo[KP];
             const float n = centre_split<D, KP>(x, o, hi, lo);
-            store_row<KP>(s_b[0][0], kN, lane, hi);
-            store_row<KP>(s_b[0][1], kN, lane, lo);
-            s_ni[0][lane] = n;
-            s_nneg[0][lane] = -n;
+            store_row<KP>(s_b[0], kN, lane, hi);
+            store_row<KP>(s_b[1], kN, lane, lo);
+            s_ni[lane] = n;
+            s_nneg[lane] = -n;
             float nm = lane < cnt ? n : 0.0f;
 #pragma unroll
             for (int s = 16; s > 0; s >>= 1) nm = fmaxf(nm, __shfl_xor_sync(kFull, nm, s));
@@ -527,9 +526,9 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
         const int n_tiles = (total + kM - 1) / kM;
         unsigned act = cnt >= kN ? kFull : ((1u << cnt) - 1u);
         int run = 0, totals = 0;  // lane c: this warp's hits of column c; all warps' hits after the last tile
-        // Columns: column c holds item point pcol (of lane c) in point set `set`; ncols
+        // Columns: column c (row c of s_b, s_x, s_ni) holds item point pcol (of lane c); ncols
         // columns hold points.  narrow: the MMA computes 16 columns (N = 16).
-        int set = 0, ncols = cnt, pcol = lane;
+        int ncols = cnt, pcol = lane;
         bool narrow = false;
 
         // One candidate row per thread.  fetch: the row's point index (a cursor over
@@ -569,7 +568,7 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
             const int b = t & 1;
             const uint32_t d = tmem + (uint32_t)(b * kN);
             const uint32_t ah = smem_u32(s_a[b][0]), al = smem_u32(s_a[b][1]);
-            const uint32_t bh = smem_u32(s_b[set][0]), bl = smem_u32(s_b[set][1]);
+            const uint32_t bh = smem_u32(s_b[0]), bl = smem_u32(s_b[1]);
             const uint32_t id = narrow ? kIdescNarrow : kIdesc;
 #pragma unroll
             for (int s = 0; s < KP / 8; ++s) {
@@ -610,16 +609,16 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
                 unsigned mlo, mhi;  // bit c: v_c > tlo, v_c > thi
                 if (narrow) {
                     tmem_ld16(taddr, g);
-                    classify<kN / 2>(g, s_nneg[1], tlo_cur, thi_cur, mlo, mhi);
+                    classify<kN / 2>(g, s_nneg, tlo_cur, thi_cur, mlo, mhi);
                 } else {
                     tmem_ld32(taddr, g);
-                    classify<kN>(g, s_nneg[set], tlo_cur, thi_cur, mlo, mhi);
+                    classify<kN>(g, s_nneg, tlo_cur, thi_cur, mlo, mhi);
                 }
-                const float *sx = s_x[set];
+                const float *sx = s_x;
                 unsigned hb = ~mlo & act;
                 unsigned bb = ~mhi & mlo & act;
                 if constexpr (AUDIT)
-                    audit_tile<D>(sx, s_ni[set], g, act, hb, bb, j_cur, nj_cur, xs, e2j, kap, audit);
+                    audit_tile<D>(sx, s_ni, g, act, hb, bb, j_cur, nj_cur, xs, e2j, kap, audit);
                 if (__any_sync(kFull, bb != 0)) {
                     if (bb) {
                         float xj[D];
@@ -660,10 +659,13 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
             if (early && !act) break;
             if (t < n_tiles) {
                 // Packing (early exit only, once per item): when at most 16 columns are
-                // still active, they move to the first 16 columns of point set 1 and the
-                // MMAs compute N = 16 from then on, halving the classification.  A finished
-                // column's count is final: it is written out here.  No MMA is in flight
-                // (the last one was waited for above), so set 1 may be written.
+                // still active, they move to the first 16 rows of the item's operand and
+                // the MMAs compute N = 16 from then on, halving the classification.  A
+                // finished column's count is final: it is written out here.  No MMA is in
+                // flight (the last one was waited for above), so the operand may be
+                // rewritten; warp 1 moves the rows through the candidate buffer of the
+                // tile before this one (its MMA is complete, and it is next staged after
+                // the following barrier), so only warp 1 touches them meanwhile.
                 if (early && !narrow && __popc(act) <= kN / 2) {
                     const int nk = __popc(act);
                     if (warp == 0 && lane < ncols && !((act >> lane) & 1u)) nn_sorted[p0 + pcol] = totals;
@@ -675,22 +677,40 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
                         const int ln = s_listn[src];
                         __syncwarp();
                         s_listn[lane] = ln;
-                    } else if (warp == 1 && lane < nk) {
-#pragma unroll
-                        for (int q = 0; q < KC; ++q)
+                    } else if (warp == 1) {
+                        constexpr int TS = 2 * KC * 4 + P + 4;  // words per row in the buffer (16-byte multiple)
+                        uint32_t *tmp = &s_a[(t + 1) & 1][0][0] + lane * TS;
+                        if (lane < nk) {
 #pragma unroll
                             for (int h = 0; h < 2; ++h)
-                                *reinterpret_cast<uint4 *>(&s_b[1][h][(q * kN + lane) * 4]) =
-                                    *reinterpret_cast<const uint4 *>(&s_b[0][h][(q * kN + src) * 4]);
 #pragma unroll
-                        for (int q = 0; q < P / 4; ++q)
-                            *reinterpret_cast<float4 *>(&s_x[1][lane * P + 4 * q]) =
-                                *reinterpret_cast<const float4 *>(&s_x[0][src * P + 4 * q]);
-                        s_ni[1][lane] = s_ni[0][src];
-                        s_nneg[1][lane] = s_nneg[0][src];
-                        fence_async_smem();
+                                for (int q = 0; q < KC; ++q)
+                                    *reinterpret_cast<uint4 *>(tmp + (h * KC + q) * 4) =
+                                        *reinterpret_cast<const uint4 *>(&s_b[h][(q * kN + src) * 4]);
+#pragma unroll
+                            for (int q = 0; q < P / 4; ++q)
+                                *reinterpret_cast<float4 *>(tmp + 2 * KC * 4 + 4 * q) =
+                                    *reinterpret_cast<const float4 *>(&s_x[src * P + 4 * q]);
+                            tmp[2 * KC * 4 + P] = __float_as_uint(s_ni[src]);
+                            tmp[2 * KC * 4 + P + 1] = __float_as_uint(s_nneg[src]);
+                        }
+                        __syncwarp();
+                        if (lane < nk) {
+#pragma unroll
+                            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                                for (int q = 0; q < KC; ++q)
+                                    *reinterpret_cast<uint4 *>(&s_b[h][(q * kN + lane) * 4]) =
+                                        *reinterpret_cast<const uint4 *>(tmp + (h * KC + q) * 4);
+#pragma unroll
+                            for (int q = 0; q < P / 4; ++q)
+                                *reinterpret_cast<float4 *>(&s_x[lane * P + 4 * q]) =
+                                    *reinterpret_cast<const float4 *>(tmp + 2 * KC * 4 + 4 * q);
+                            s_ni[lane] = __uint_as_float(tmp[2 * KC * 4 + P]);
+                            s_nneg[lane] = __uint_as_float(tmp[2 * KC * 4 + P + 1]);
+                            fence_async_smem();
+                        }
                     }
-                    set = 1;
                     narrow = true;
                     ncols = nk;
                     act = (1u << nk) - 1u;
