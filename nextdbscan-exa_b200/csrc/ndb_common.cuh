@@ -166,6 +166,27 @@ __device__ __forceinline__ int uf_find_ro(const int *parent, int x, int *err) {
     return x;
 }
 
+// Union of the components of a and b; returns the root they share afterwards (as
+// of the hook: later unions may hang it under a smaller root, so it stays an
+// ancestor of both, and a later find from it is a shortcut from a or b).
+__device__ __forceinline__ int uf_union_root(int *parent, int a, int b, int *err) {
+    const int lim = uf_limit(err);
+    for (int it = 0; it < lim; ++it) {
+        a = uf_find(parent, a, err);
+        b = uf_find(parent, b, err);
+        if (a == b) return a;
+        if (a > b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        const int old = atomicCAS(parent + b, b, a);
+        if (old == b) return a;
+    }
+    atomicExch(err, 1);
+    return a;
+}
+
 __device__ __forceinline__ void uf_union(int *parent, int a, int b, int *err) {
     const int lim = uf_limit(err);
     for (int it = 0; it < lim; ++it) {

@@ -1319,18 +1319,14 @@ __global__ void __launch_bounds__(kCountWarps * kWarp) union_points_kernel(
                 bool hit = false;
                 if (__any_sync(kFull, want && len <= e2)) hit = want && dist_part<D, H, D>(xi, xj, len) <= e2;
                 tested += want ? 1 : 0;
-                if (hit) {
-                    uf_union(parent, ik, j, err);
-                    pj = uf_find(parent, j, err);
-                }
+                // finds from known ancestors: the core's root snapshot and pj; the
+                // shared root that comes back is again an ancestor of j
+                if (hit) pj = uf_union_root(parent, sroot[k], pj, err);
             } else if (valid && j > ik && sroot[k] != pj) {
                 float xi[D];
                 load_point_smem<D>(si + k * P, xi);
                 ++tested;
-                if (in_range<D>(xi, xj, e2)) {
-                    uf_union(parent, ik, j, err);
-                    pj = uf_find(parent, j, err);
-                }
+                if (in_range<D>(xi, xj, e2)) pj = uf_union_root(parent, sroot[k], pj, err);
             }
         }
         pairs += (unsigned long long)__reduce_add_sync(kFull, (unsigned)tested);
@@ -1443,11 +1439,14 @@ __global__ void union_lists_kernel(int64_t nv, const int32_t *__restrict__ nn_so
     if (cell_units && skip_dense && cell_start[a + 1] - cell_start[a] >= min_pts) return;
     const int len = min(min(nn_sorted[s], cap), kListUnions);
     const int32_t *l = nbr_list + s * list_stride;
+    // every union starts its find from the root the previous one left (an ancestor
+    // of a), not from a itself
+    int ra = a;
     for (int q = 0; q < len; ++q) {
         const int j = l[q];
         if (j == (int)s || !core_sorted[j]) continue;
         const int b = cell_units ? pcell[j] : j;
-        if (a != b) uf_union(parent, a, b, err);
+        if (a != b) ra = uf_union_root(parent, ra, b, err);
     }
 }
 
