@@ -1806,10 +1806,39 @@ __global__ void bbox_batch_init_kernel(int *lo_hi, int d, int n_jobs, unsigned l
     if (i < n_jobs) n_invalid[i] = 0ull;
 }
 
+// One point's coordinates: 16-byte vector loads when a point's row is a multiple of
+// 16 bytes (d % 4 == 0; rows then start 16-byte aligned), 8-byte ones at d = 2.
+template <int D>
+__device__ __forceinline__ void load_row(const float *__restrict__ p, float (&x)[D]) {
+    if constexpr (D % 4 == 0) {
+#pragma unroll
+        for (int q = 0; q < D / 4; ++q) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(p) + q);
+            x[4 * q + 0] = v.x;
+            x[4 * q + 1] = v.y;
+            x[4 * q + 2] = v.z;
+            x[4 * q + 3] = v.w;
+        }
+    } else if constexpr (D == 2) {
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+        x[0] = v.x;
+        x[1] = v.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < D; ++k) x[k] = __ldg(p + k);
+    }
+}
+
+// Per-job bounding boxes (ordered-int min/max per dimension) and invalid-point counts
+// of a batch: blocks (x, job).  Warps reduce by shuffles, the block through shared
+// memory, and one lane per dimension and bound issues the block's atomic.
 template <int D>
 __global__ void __launch_bounds__(kBlock) bbox_batch_kernel(const float *__restrict__ coords,
                                                             const JobDev *__restrict__ jobs, int *lo_hi,
                                                             unsigned long long *n_invalid) {
+    constexpr int W = kBlock / 32;
+    __shared__ int s_lh[W][2 * D];
+    __shared__ unsigned s_bad[W];
     const int j = blockIdx.y;
     const JobDev &J = jobs[j];
     int lo[D], hi[D];
@@ -1820,10 +1849,8 @@ __global__ void __launch_bounds__(kBlock) bbox_batch_kernel(const float *__restr
     }
     unsigned bad = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < J.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float *p = coords + (J.off + i) * D;
         float x[D];
-#pragma unroll
-        for (int k = 0; k < D; ++k) x[k] = p[k];
+        load_row<D>(coords + (J.off + i) * D, x);
         bool ok = x[0] != FLT_MAX;
 #pragma unroll
         for (int k = 0; k < D; ++k) ok = ok && isfinite(x[k]);
@@ -1840,22 +1867,35 @@ __global__ void __launch_bounds__(kBlock) bbox_batch_kernel(const float *__restr
     }
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            lo[k] = min(lo[k], __shfl_xor_sync(kFull, lo[k], o));
-            hi[k] = max(hi[k], __shfl_xor_sync(kFull, hi[k], o));
-        }
+        lo[k] = __reduce_min_sync(kFull, lo[k]);
+        hi[k] = __reduce_max_sync(kFull, hi[k]);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(kFull, bad, o);
-    if ((threadIdx.x & 31) == 0) {
-        int *lh = lo_hi + (int64_t)j * 2 * D;
+    bad = __reduce_add_sync(kFull, bad);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
 #pragma unroll
         for (int k = 0; k < D; ++k) {
-            if (lo[k] != 0x7fffffff) atomicMin(lh + k, lo[k]);
-            if (hi[k] != (int)0x80000000) atomicMax(lh + D + k, hi[k]);
+            s_lh[w][k] = lo[k];
+            s_lh[w][D + k] = hi[k];
         }
-        if (bad) atomicAdd(n_invalid + j, (unsigned long long)bad);
+        s_bad[w] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * D) {
+        const int t = threadIdx.x;
+        int v = s_lh[0][t];
+        for (int q = 1; q < W; ++q) v = t < D ? min(v, s_lh[q][t]) : max(v, s_lh[q][t]);
+        int *lh = lo_hi + (int64_t)j * 2 * D;
+        if (t < D) {
+            if (v != 0x7fffffff) atomicMin(lh + t, v);
+        } else {
+            if (v != (int)0x80000000) atomicMax(lh + t, v);
+        }
+    }
+    if (threadIdx.x == 0) {
+        unsigned b = 0;
+        for (int q = 0; q < W; ++q) b += s_bad[q];
+        if (b) atomicAdd(n_invalid + j, (unsigned long long)b);
     }
 }
 
@@ -1869,7 +1909,12 @@ __global__ void __launch_bounds__(kBlock) key_batch_kernel(const float *__restri
         const int64_t o = J.off + i;
         const float *p = coords + o * D;
         K key = invalid_key;
-        if (point_valid<D>(p)) {
+        float x[D];  // validity from one vector load of the row; the gridded coordinates are re-read (L1)
+        load_row<D>(p, x);
+        bool ok = x[0] != FLT_MAX;
+#pragma unroll
+        for (int k = 0; k < D; ++k) ok = ok && isfinite(x[k]);
+        if (ok) {
             unsigned long long kk = J.key_base;
 #pragma unroll
             for (int a = 0; a < kMaxGridDims; ++a)
