@@ -1706,6 +1706,7 @@ __global__ void output_ci_kernel(const int32_t *__restrict__ ci_sorted, int64_t 
     // windows as in scatter_nn_kernel; every point is counted in its own window only
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned noise = 0, roots = 0;
+    int job = -1;  // batched runs: the point's job, whose counters take its noise and roots
     const int32_t o = s < n ? __ldcs(perm + s) : 0;
     if (s < n && o >= win_lo && o < win_hi) {
         int32_t v;
@@ -1720,17 +1721,25 @@ __global__ void output_ci_kernel(const int32_t *__restrict__ ci_sorted, int64_t 
         noise = v == kNoCluster;
         if (jobs) {
             // ids are ranks among all cores of the batch: make them ranks within the job
-            const int j = job_of_point(jobs, n_jobs, o);
-            const JobDev &J = jobs[j];
+            job = job_of_point(jobs, n_jobs, o);
+            const JobDev &J = jobs[job];
             if (v != kNoCluster) v -= core_rank(core_bits, core_prefix, (int32_t)J.off);
             if (J.ci_out) J.ci_out[o - J.off] = v;
-            if (noise) atomicAdd(job_counters + 4 * j + 1, 1ull);
-            if (roots) atomicAdd(job_counters + 4 * j, 1ull);
-            noise = 0;
-            roots = 0;
         } else if (out) {
             out[o] = v;
         }
+    }
+    if (jobs) {
+        // per-job counters: the lanes of one job (sorted points are grouped by job,
+        // so usually the whole warp) add their noise and roots with one atomic each
+        const unsigned peers = __match_any_sync(kFull, job);
+        const unsigned nm = __ballot_sync(kFull, noise != 0) & peers, rm = __ballot_sync(kFull, roots != 0) & peers;
+        if (job >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+            if (nm) atomicAdd(job_counters + 4 * job + 1, (unsigned long long)__popc(nm));
+            if (rm) atomicAdd(job_counters + 4 * job, (unsigned long long)__popc(rm));
+        }
+        noise = 0;
+        roots = 0;
     }
     noise = __reduce_add_sync(kFull, noise);
     roots = __reduce_add_sync(kFull, roots);
