@@ -464,8 +464,10 @@ __global__ void __launch_bounds__(kThreads, TcBlocks<D>::v) count_tc_kernel(
         int cnt, jb = -1;
         if (rec) {
             const bool ok = mbar_wait(&s_rbar[slot], (rphase >> slot) & 1u);
-            rphase ^= 1u << slot;
-            rpend &= ~(1u << slot);
+            if (ok) {  // else the copy may still be in flight: the exit waits for it
+                rphase ^= 1u << slot;
+                rpend &= ~(1u << slot);
+            }
             if (__syncthreads_or(!ok)) {
                 if (tid == 0) {
                     s_abort = 1;
